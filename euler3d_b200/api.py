@@ -1,0 +1,423 @@
+"""Python face of the B200 residual/update path.
+
+Two layers over the C ABI (include/e3d.h):
+
+* ``Case`` / ``Solver``: load the reference's deck + topology + SU2 blocks,
+  create a device-resident solver, run fused outer iterations, read results.
+* Strategy classes with the reference's names and call structure
+  (FluxScheme/RoeScheme/AusmScheme, Gradient/GreenGauss/LeastSquares,
+  Limiter/BarthJespersen/Venkatakrishnan, Interpolation/FirstOrder/SecondOrder,
+  Timestep, Updater, ResidualCalculator, RungeKutta, ReferenceSolver), selected
+  by the same strings (Solver/src/ResidualCalculator.cpp:72-95,
+  Solver/src/SecondOrder.cpp:50-61).  Each method launches the matching
+  granular kernel on a device-resident ``Block``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _lib as L
+
+_ARRAYS_ALL5 = ("prim", "limiter")
+_ARRAYS_REAL5 = ("conv_res", "diss_res", "w0")
+_ARRAYS_REAL1 = ("dt", "spectral_radius")
+
+
+class Case:
+    """Host case: the reference's Interface + CompleteMesh after InitializeMyBlocks."""
+
+    def __init__(self, deck_path: str, workdir: str | None = None):
+        lib = L.lib()
+        h = C.c_void_p()
+        wd = workdir if workdir is not None else os.path.dirname(os.path.abspath(deck_path))
+        L.check(lib.e3d_case_load(deck_path.encode(), wd.encode(), C.byref(h)))
+        self._h = h
+        n = C.c_int()
+        L.check(lib.e3d_case_n_blocks(h, C.byref(n)))
+        self.n_blocks = n.value
+        d = L.DeckInfo()
+        L.check(lib.e3d_case_deck(h, C.byref(d)))
+        self.deck = d
+
+    def block_info(self, b: int) -> L.BlockInfo:
+        info = L.BlockInfo()
+        L.check(L.lib().e3d_case_block_info(self._h, b, C.byref(info)))
+        return info
+
+    def get(self, b: int, name: str) -> np.ndarray:
+        lib = L.lib()
+        n = C.c_int64()
+        f64 = name in ("face_normal", "face_area", "face_center", "r_left", "r_right", "cell_volume",
+                       "cell_center", "ls_weights", "node_xyz")
+        fn = lib.e3d_case_get_f64 if f64 else lib.e3d_case_get_i32
+        L.check(fn(self._h, b, name.encode(), None, C.byref(n)))
+        out = np.empty(n.value, dtype=np.float64 if f64 else np.int32)
+        L.check(fn(self._h, b, name.encode(), L.ptr(out), C.byref(n)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().e3d_case_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """Device-resident solver over every block of a case."""
+
+    def __init__(self, case: Case, precision: str = "fp64", carry_w0: int = -1, use_graph: bool = True,
+                 device: int = -1, stream: int | None = None, hist_capacity: int = 4096):
+        lib = L.lib()
+        o = L.Options()
+        lib.e3d_default_options(C.byref(o))
+        o.precision = L.FP32 if precision == "fp32" else L.FP64
+        o.carry_w0 = carry_w0
+        o.use_graph = 1 if use_graph else 0
+        o.device = device
+        o.stream = stream
+        o.hist_capacity = hist_capacity
+        h = C.c_void_p()
+        L.check(lib.e3d_solver_create(case._h, C.byref(o), C.byref(h)))
+        self._h = h
+        self.case = case
+        self.precision = precision
+        self.n_blocks = case.n_blocks
+        self._info = [case.block_info(b) for b in range(case.n_blocks)]
+
+    # ---- fused outer iterations
+    def iterate(self, n: int) -> None:
+        L.check(L.lib().e3d_iterate(self._h, n))
+
+    def solve(self, max_iter: int, criterion: float, check_every: int = 1) -> int:
+        done = C.c_int()
+        L.check(L.lib().e3d_solve(self._h, max_iter, criterion, check_every, C.byref(done)))
+        return done.value
+
+    def sync(self) -> None:
+        L.check(L.lib().e3d_solver_sync(self._h))
+
+    def history(self) -> dict[str, np.ndarray]:
+        lib = L.lib()
+        n = C.c_int()
+        L.check(lib.e3d_history_length(self._h, C.byref(n)))
+        recs = (L.IterRecord * max(1, n.value))()
+        if n.value:
+            L.check(lib.e3d_history(self._h, 0, n.value, C.cast(recs, C.c_void_p)))
+        r = recs[:n.value]
+        return {
+            "iter": np.array([x.iter for x in r], dtype=np.int64),
+            "rms": np.array([list(x.rms) for x in r]).reshape(-1, 5),
+            "conv": np.array([list(x.conv) for x in r]).reshape(-1, 5),
+            "cl": np.array([x.cl for x in r]), "cd": np.array([x.cd for x in r]),
+            "cmx": np.array([x.cmx for x in r]), "cmy": np.array([x.cmy for x in r]),
+            "cmz": np.array([x.cmz for x in r]),
+        }
+
+    # ---- state
+    def _len(self, b: int, name: str) -> int:
+        i = self._info[b]
+        if name in _ARRAYS_ALL5:
+            return 5 * i.n_all
+        if name == "grad":
+            return 15 * i.n_all
+        if name in _ARRAYS_REAL5:
+            return 5 * i.n_real
+        if name in _ARRAYS_REAL1:
+            return i.n_real
+        raise KeyError(name)
+
+    def get(self, b: int, name: str) -> np.ndarray:
+        out = np.empty(self._len(b, name), dtype=np.float64)
+        L.check(L.lib().e3d_state_get(self._h, b, name.encode(), L.ptr(out), out.size))
+        return out
+
+    def set(self, b: int, name: str, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        L.check(L.lib().e3d_state_set(self._h, b, name.encode(), L.ptr(a), a.size))
+
+    def flow_data(self) -> np.ndarray:
+        out = np.empty(10 * self.n_blocks, dtype=np.float64)
+        L.check(L.lib().e3d_flow_data(self._h, L.ptr(out), out.size))
+        return out.reshape(self.n_blocks, 10)
+
+    def device_bytes(self) -> int:
+        n = C.c_int64()
+        L.check(L.lib().e3d_solver_device_bytes(self._h, C.byref(n)))
+        return n.value
+
+    def launches_per_iteration(self) -> int:
+        n = C.c_int()
+        L.check(L.lib().e3d_launches_per_iteration(self._h, C.byref(n)))
+        return n.value
+
+    def time_kernels(self, n_iter: int) -> list[dict]:
+        rows = C.c_int()
+        names = C.create_string_buffer(1024)
+        launches = np.zeros(32, dtype=np.int32)
+        ms = np.zeros(32)
+        by = np.zeros(32)
+        L.check(L.lib().e3d_time_kernels(self._h, n_iter, names, 1024, L.ptr(launches), L.ptr(ms), L.ptr(by), 32,
+                                         C.byref(rows)))
+        nm = names.value.decode().split(",")
+        return [{"name": nm[i], "launches": int(launches[i]), "total_ms": float(ms[i]),
+                 "bytes_per_launch": float(by[i])} for i in range(rows.value)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().e3d_solver_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------------
+# Strategy classes with the reference's names.  A ``Block`` is one block of a
+# device-resident solver (the reference's Block*); methods launch one kernel.
+class Block:
+    def __init__(self, solver: Solver, block_id: int):
+        self.solver = solver
+        self.block_id_ = block_id
+
+    @property
+    def _h(self):
+        return self.solver._h
+
+
+class FluxScheme:
+    """Solver/head/FluxScheme.h:9-23."""
+
+    _scheme = None
+
+    def __init__(self, gamma: float):
+        self.gamma_ = gamma
+        self.current_beta_ = 1.0
+
+    def computeFluxConv(self, block: Block) -> None:
+        L.check(L.lib().e3d_flux_conv(block._h, block.block_id_, self._scheme))
+
+    def computeFluxDiss(self, block: Block) -> None:
+        L.check(L.lib().e3d_flux_diss(block._h, block.block_id_, self._scheme, self.current_beta_))
+
+
+class RoeScheme(FluxScheme):
+    """Central flux + Roe dissipation (FluxScheme.cpp:16-211, RoeScheme.cpp:12-311)."""
+
+    _scheme = L.FLUX["roe"]
+
+
+class AusmScheme(FluxScheme):
+    """Liou-Steffen AUSM (AusmScheme.cpp:12-243, :647-871)."""
+
+    _scheme = L.FLUX["ausm"]
+
+
+class Gradient:
+    _kind = None
+
+    def computeGradients(self, block: Block) -> None:
+        L.check(L.lib().e3d_gradients(block._h, block.block_id_, self._kind))
+
+
+class GreenGauss(Gradient):
+    _kind = L.GRAD["greengauss"]
+
+
+class LeastSquares(Gradient):
+    _kind = L.GRAD["leastsquares"]
+
+
+class Limiter:
+    _kind = None
+    omega_ = 0.0
+    k_ = 0.0
+
+    def computeLimiters(self, block: Block) -> None:
+        L.check(L.lib().e3d_limiters(block._h, block.block_id_, self._kind, self.omega_, self.k_))
+
+
+class BarthJespersen(Limiter):
+    _kind = L.LIM["barthjespersen"]
+
+    def __init__(self, omega: float):
+        self.omega_ = omega
+
+
+class Venkatakrishnan(Limiter):
+    _kind = L.LIM["venkatakrishnan"]
+
+    def __init__(self, k: float):
+        self.k_ = k
+
+
+class Interpolation:
+    def computeInterpolation(self, block: Block) -> None:
+        raise NotImplementedError
+
+
+class FirstOrder(Interpolation):
+    """No reconstruction (FirstOrder.cpp:12-15)."""
+
+    def computeInterpolation(self, block: Block) -> None:
+        return None
+
+
+class SecondOrder(Interpolation):
+    """Gradient then limiter (SecondOrder.cpp:20-61): 'leastsquares' else
+    Green-Gauss; 'venkatakrishnan' else Barth-Jespersen."""
+
+    def __init__(self, gradient_choice: str, limiter_choice: str, omega: float, k: float):
+        self.gradient_ = LeastSquares() if gradient_choice == "leastsquares" else GreenGauss()
+        self.limiter_ = Venkatakrishnan(k) if limiter_choice == "venkatakrishnan" else BarthJespersen(omega)
+
+    def computeInterpolation(self, block: Block) -> None:
+        self.gradient_.computeGradients(block)
+        self.limiter_.computeLimiters(block)
+
+
+class NoSmoother:
+    def smoothResidual(self, block: Block) -> None:
+        return None
+
+
+RK_TABLES = {  # Solver/src/RungeKutta.cpp:23-68
+    1: ([1.0], [1.0]),
+    2: ([0.6, 1.0], [1.0, 0.0]),
+    3: ([0.6, 0.6, 1.0], [1.0, 0.0, 0.0]),
+    4: ([0.25, 1.0 / 3.0, 0.5, 1.0], [1.0, 0.5, 0.0, 0.0]),
+    5: ([0.2742, 0.2067, 0.5020, 0.5142, 1.0], [1.0, 0.0, 0.56, 0.0, 0.44]),
+}
+
+
+class ResidualCalculator:
+    """ResidualCalculator.cpp:24-95."""
+
+    def __init__(self, gamma, beta_rk, interpolation_choice, gradient_choice, limiter_choice,
+                 flux_scheme_choice, residual_smoother_choice, omega, k):
+        self.current_stage_ = 0
+        self.beta_rk_ = list(beta_rk)
+        self.interpolation_ = (SecondOrder(gradient_choice, limiter_choice, omega, k)
+                               if interpolation_choice == 2 else FirstOrder())
+        if flux_scheme_choice == "roe":
+            self.flux_scheme_ = RoeScheme(gamma)
+        elif flux_scheme_choice == "ausm":
+            self.flux_scheme_ = AusmScheme(gamma)
+        else:
+            raise ValueError(f"unknown flux scheme {flux_scheme_choice!r} (roe|ausm)")
+        if residual_smoother_choice:
+            raise ValueError("implicit residual smoothing is not provided by this path")
+        self.residual_smoother_ = NoSmoother()
+
+    def computeResidual(self, block: Block) -> None:
+        self.interpolation_.computeInterpolation(block)
+        self.flux_scheme_.computeFluxConv(block)
+        self.flux_scheme_.current_beta_ = self.beta_rk_[self.current_stage_]
+        # the reference guard `beta > (10^-16)` is an integer XOR (== -6): always true
+        self.flux_scheme_.computeFluxDiss(block)
+        self.residual_smoother_.smoothResidual(block)
+
+
+class Updater:
+    """Updater.cpp:12-88."""
+
+    def __init__(self, gamma, alpha_rk):
+        self.gamma_ = gamma
+        self.alpha_rk_ = list(alpha_rk)
+        self.current_stage_ = 0
+
+    def updateInternalBlock(self, block: Block) -> None:
+        L.check(L.lib().e3d_update_internal(block._h, block.block_id_, self.alpha_rk_[self.current_stage_]))
+
+    def updateBoundary(self, block: Block) -> None:
+        L.check(L.lib().e3d_update_boundary(block._h, block.block_id_))
+
+
+class Timestep:
+    """Timestep.cpp:26-148."""
+
+    def __init__(self, gamma, cfl):
+        self.gamma_ = gamma
+        self.cfl_ = cfl
+
+    def computeSpectralRadius(self, block: Block) -> None:
+        L.check(L.lib().e3d_spectral_radius(block._h, block.block_id_))
+
+    def computeTimestep(self, block: Block) -> None:
+        L.check(L.lib().e3d_timestep(block._h, block.block_id_))
+
+
+class RungeKutta:
+    """RungeKutta.cpp:15-94."""
+
+    def __init__(self, gamma, stage_number, interpolation_choice, gradient_choice, limiter_choice,
+                 flux_scheme_choice, residual_smoother_choice, omega, k):
+        if stage_number not in RK_TABLES:
+            raise ValueError("Invalid number of RK stages")
+        self.stage_number_ = stage_number
+        alpha, beta = RK_TABLES[stage_number]
+        self.updater_ = Updater(gamma, alpha)
+        self.residual_calculator_ = ResidualCalculator(gamma, beta, interpolation_choice, gradient_choice,
+                                                       limiter_choice, flux_scheme_choice,
+                                                       residual_smoother_choice, omega, k)
+
+    def computeRungeKutta(self, block: Block) -> None:
+        for s in range(self.stage_number_):
+            self.residual_calculator_.current_stage_ = s
+            self.residual_calculator_.computeResidual(block)
+            self.updater_.current_stage_ = s
+            self.updater_.updateInternalBlock(block)
+            self.updater_.updateBoundary(block)
+
+
+def save_w0(block: Block) -> None:
+    """Solver::saveW0 (Solver.cpp:161-210)."""
+    L.check(L.lib().e3d_save_w0(block._h, block.block_id_))
+
+
+def halo(solver: Solver) -> None:
+    """BlockCommunicator::updateBoundaries (MPI/src/BlockCommunicator.cpp:66-270)."""
+    L.check(L.lib().e3d_halo(solver._h))
+
+
+class ReferenceSolver:
+    """Solver::solve (Solver.cpp:36-98) sequenced call by call through the strategy
+    objects, block after block, on the device.  ``iterate`` runs n outer
+    iterations and returns the per-block flow data after each one."""
+
+    def __init__(self, solver: Solver):
+        d = solver.case.deck
+        self.solver = solver
+        self.timestep_ = Timestep(d.gamma, d.cfl)
+        grad = "leastsquares" if d.gradient == L.GRAD["leastsquares"] else "greengauss"
+        lim = "venkatakrishnan" if d.limiter == L.LIM["venkatakrishnan"] else "barthjespersen"
+        flux = {0: "roe", 1: "ausm"}[d.flux]
+        self.runge_kutta_ = RungeKutta(d.gamma, d.stages, d.order, grad, lim, flux, bool(d.smoothing),
+                                       d.omega, d.k)
+        self.blocks = [Block(solver, b) for b in range(solver.n_blocks)]
+        self._started = False
+
+    def iterate(self, n: int) -> list[np.ndarray]:
+        if not self._started:
+            halo(self.solver)
+            self._started = True
+        out = []
+        for _ in range(n):
+            for b in self.blocks:
+                save_w0(b)
+                self.timestep_.computeSpectralRadius(b)
+                self.timestep_.computeTimestep(b)
+                self.runge_kutta_.computeRungeKutta(b)
+            out.append(self.solver.flow_data())
+            halo(self.solver)
+        return out

@@ -1,0 +1,338 @@
+// extern "C" boundary: status codes, thread-local error text, no exceptions
+// crossing the ABI.
+#include "../../include/e3d.h"
+
+#include <cstring>
+#include <string>
+
+#include "engine.hpp"
+#include "mesh.hpp"
+
+struct e3d_case {
+	e3d::HostCase hc;
+};
+struct e3d_solver {
+	std::unique_ptr<e3d::Engine> eng;
+};
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+	g_err = msg;
+	return code;
+}
+
+template <class F>
+int guard(F&& f) {
+	try {
+		f();
+		g_err.clear();
+		return E3D_OK;
+	} catch (const e3d::Error& e) {
+		return fail(e.code, e.what());
+	} catch (const std::bad_alloc&) {
+		return fail(E3D_ERR_LIMIT, "host allocation failed");
+	} catch (const std::exception& e) {
+		return fail(E3D_ERR_STATE, e.what());
+	}
+}
+
+const e3d::HostBlock& block_of(const e3d_case* c, int b) {
+	if (!c) throw e3d::Error(E3D_ERR_ARG, "null case");
+	if (b < 0 || b >= (int)c->hc.blocks.size()) throw e3d::Error(E3D_ERR_ARG, "block index out of range");
+	return c->hc.blocks[b];
+}
+
+e3d::Engine& eng(e3d_solver* s) {
+	if (!s || !s->eng) throw e3d::Error(E3D_ERR_ARG, "null solver");
+	return *s->eng;
+}
+}  // namespace
+
+extern "C" {
+
+const char* e3d_last_error(void) { return g_err.c_str(); }
+const char* e3d_version(void) { return "euler3d_b200 0.1 (sm_100a)"; }
+
+void e3d_default_options(e3d_options* o) {
+	if (!o) return;
+	o->precision = E3D_FP64;
+	o->carry_w0 = -1;
+	o->use_graph = 1;
+	o->device = -1;
+	o->stream = nullptr;
+	o->hist_capacity = 4096;
+}
+
+int e3d_case_load(const char* deck_path, const char* workdir, e3d_case** out) {
+	if (!deck_path || !out) return fail(E3D_ERR_ARG, "null argument");
+	*out = nullptr;
+	return guard([&] {
+		auto* c = new e3d_case;
+		try {
+			c->hc = e3d::load_case(deck_path, workdir ? workdir : "");
+		} catch (...) {
+			delete c;
+			throw;
+		}
+		*out = c;
+	});
+}
+
+int e3d_case_free(e3d_case* c) {
+	delete c;
+	return E3D_OK;
+}
+
+int e3d_case_deck(const e3d_case* c, e3d_deck_info* o) {
+	if (!c || !o) return fail(E3D_ERR_ARG, "null argument");
+	const e3d::Deck& d = c->hc.deck;
+	o->cfl = d.cfl;
+	o->gamma = d.gamma;
+	o->aoa_deg = d.aoa_deg;
+	o->mach = d.mach;
+	o->cmac = d.cmac;
+	o->criterion = d.criterion;
+	o->omega = d.omega;
+	o->k = d.k;
+	o->stages = d.stages;
+	o->max_iter = d.max_iter;
+	o->smoothing = d.smoothing ? 1 : 0;
+	o->order = d.order;
+	o->flux = d.flux == "roe" ? E3D_FLUX_ROE : d.flux == "ausm" ? E3D_FLUX_AUSM : -1;
+	o->gradient = d.gradient == "leastsquares" ? E3D_GRAD_LEAST_SQUARES : E3D_GRAD_GREEN_GAUSS;
+	o->limiter = d.limiter == "venkatakrishnan" ? E3D_LIM_VENKATAKRISHNAN : E3D_LIM_BARTH_JESPERSEN;
+	return E3D_OK;
+}
+
+int e3d_case_n_blocks(const e3d_case* c, int* n) {
+	if (!c || !n) return fail(E3D_ERR_ARG, "null argument");
+	*n = (int)c->hc.blocks.size();
+	return E3D_OK;
+}
+
+int e3d_case_block_info(const e3d_case* c, int block, e3d_block_info* o) {
+	if (!o) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		const e3d::HostBlock& B = block_of(c, block);
+		o->n_real = B.n_real;
+		o->n_all = B.n_all;
+		o->n_faces = B.n_faces;
+		o->n_nodes = B.n_nodes;
+		o->n_markers = (int)B.markers.size();
+		o->n_real_boundaries = B.n_real_boundaries;
+		o->n_wall_faces = (int)B.wall_faces.size();
+	});
+}
+
+int e3d_case_get_f64(const e3d_case* c, int block, const char* name, double* dst, int64_t* count) {
+	if (!name || !count) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		const e3d::HostBlock& B = block_of(c, block);
+		const std::vector<double>* v = nullptr;
+		const std::string n(name);
+		if (n == "face_normal") v = &B.face_normal;
+		else if (n == "face_area") v = &B.face_area;
+		else if (n == "face_center") v = &B.face_center;
+		else if (n == "r_left") v = &B.r_left;
+		else if (n == "r_right") v = &B.r_right;
+		else if (n == "cell_volume") v = &B.cell_volume;
+		else if (n == "cell_center") v = &B.cell_center;
+		else if (n == "ls_weights") v = &B.ls_weights;
+		else if (n == "node_xyz") v = &B.node_xyz;
+		else throw e3d::Error(E3D_ERR_ARG, "unknown float array '" + n + "'");
+		if (!dst) {
+			*count = (int64_t)v->size();
+			return;
+		}
+		if (*count != (int64_t)v->size()) throw e3d::Error(E3D_ERR_ARG, n + ": wrong count");
+		std::memcpy(dst, v->data(), v->size() * sizeof(double));
+	});
+}
+
+int e3d_case_get_i32(const e3d_case* c, int block, const char* name, int32_t* dst, int64_t* count) {
+	if (!name || !count) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		const e3d::HostBlock& B = block_of(c, block);
+		std::vector<int> tmp;
+		const std::vector<int>* v = &tmp;
+		const std::string n(name);
+		if (n == "face_cells") v = &B.face_cells;
+		else if (n == "cell_face_ptr") v = &B.cell_face_ptr;
+		else if (n == "cell_faces") v = &B.cell_faces;
+		else if (n == "cell_cells") v = &B.cell_cells;
+		else if (n == "wall_faces") v = &B.wall_faces;
+		else if (n == "face_nodes") v = &B.face_nodes;
+		else if (n == "marker_kind") {
+			for (const auto& m : B.markers) tmp.push_back(m.kind);
+		} else if (n == "marker_size") {
+			for (const auto& m : B.markers) tmp.push_back((int)m.ghosts.size());
+		} else if (n == "marker_cells") {
+			for (const auto& m : B.markers) tmp.insert(tmp.end(), m.ghosts.begin(), m.ghosts.end());
+		} else
+			throw e3d::Error(E3D_ERR_ARG, "unknown int array '" + n + "'");
+		if (!dst) {
+			*count = (int64_t)v->size();
+			return;
+		}
+		if (*count != (int64_t)v->size()) throw e3d::Error(E3D_ERR_ARG, n + ": wrong count");
+		std::memcpy(dst, v->data(), v->size() * sizeof(int));
+	});
+}
+
+int e3d_solver_create(const e3d_case* c, const e3d_options* opt, e3d_solver** out) {
+	if (!c || !out) return fail(E3D_ERR_ARG, "null argument");
+	*out = nullptr;
+	return guard([&] {
+		e3d_options o;
+		e3d_default_options(&o);
+		if (opt) o = *opt;
+		e3d::EngineOptions eo;
+		eo.precision = o.precision;
+		eo.carry_w0 = o.carry_w0;
+		eo.use_graph = o.use_graph;
+		eo.device = o.device;
+		eo.stream = static_cast<cudaStream_t>(o.stream);
+		eo.hist_capacity = o.hist_capacity > 0 ? (size_t)o.hist_capacity : 4096;
+		auto* s = new e3d_solver;
+		try {
+			s->eng.reset(new e3d::Engine(c->hc, eo));
+		} catch (...) {
+			delete s;
+			throw;
+		}
+		*out = s;
+	});
+}
+
+int e3d_solver_free(e3d_solver* s) {
+	delete s;
+	return E3D_OK;
+}
+
+int e3d_solver_sync(e3d_solver* s) { return guard([&] { eng(s).sync(); }); }
+
+int e3d_solver_device_bytes(const e3d_solver* s, int64_t* bytes) {
+	if (!s || !s->eng || !bytes) return fail(E3D_ERR_ARG, "null argument");
+	*bytes = (int64_t)s->eng->device_bytes();
+	return E3D_OK;
+}
+
+int e3d_save_w0(e3d_solver* s, int block) { return guard([&] { eng(s).save_w0(block); }); }
+int e3d_spectral_radius(e3d_solver* s, int block) { return guard([&] { eng(s).spectral_radius(block); }); }
+int e3d_timestep(e3d_solver* s, int block) { return guard([&] { eng(s).timestep(block); }); }
+int e3d_gradients(e3d_solver* s, int block, int kind) {
+	if (kind != E3D_GRAD_GREEN_GAUSS && kind != E3D_GRAD_LEAST_SQUARES) return fail(E3D_ERR_ARG, "unknown gradient kind");
+	return guard([&] { eng(s).gradients(block, kind); });
+}
+int e3d_limiters(e3d_solver* s, int block, int kind, double omega, double k) {
+	if (kind != E3D_LIM_BARTH_JESPERSEN && kind != E3D_LIM_VENKATAKRISHNAN) return fail(E3D_ERR_ARG, "unknown limiter kind");
+	return guard([&] { eng(s).limiters(block, kind, omega, k); });
+}
+int e3d_flux_conv(e3d_solver* s, int block, int scheme) {
+	if (scheme != E3D_FLUX_ROE && scheme != E3D_FLUX_AUSM) return fail(E3D_ERR_ARG, "unknown flux scheme");
+	return guard([&] { eng(s).flux_conv(block, scheme); });
+}
+int e3d_flux_diss(e3d_solver* s, int block, int scheme, double beta) {
+	if (scheme != E3D_FLUX_ROE && scheme != E3D_FLUX_AUSM) return fail(E3D_ERR_ARG, "unknown flux scheme");
+	return guard([&] { eng(s).flux_diss(block, scheme, beta); });
+}
+int e3d_update_internal(e3d_solver* s, int block, double alpha) {
+	return guard([&] { eng(s).update_internal(block, alpha); });
+}
+int e3d_update_boundary(e3d_solver* s, int block) { return guard([&] { eng(s).update_boundary(block); }); }
+int e3d_halo(e3d_solver* s) { return guard([&] { eng(s).halo(); }); }
+
+int e3d_flow_data(e3d_solver* s, double* out, int64_t count) {
+	if (!out) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		std::vector<double> v;
+		eng(s).flow_data(v);
+		if (count != (int64_t)v.size()) throw e3d::Error(E3D_ERR_ARG, "flow_data: count must be 10 * n_blocks");
+		std::memcpy(out, v.data(), v.size() * sizeof(double));
+	});
+}
+
+int e3d_iterate(e3d_solver* s, int n_iter) { return guard([&] { eng(s).iterate(n_iter); }); }
+
+int e3d_solve(e3d_solver* s, int max_iter, double criterion, int check_every, int* iters_done) {
+	return guard([&] {
+		const int n = eng(s).solve(max_iter, criterion, check_every);
+		if (iters_done) *iters_done = n;
+	});
+}
+
+int e3d_history_length(const e3d_solver* s, int* n) {
+	if (!s || !s->eng || !n) return fail(E3D_ERR_ARG, "null argument");
+	*n = (int)s->eng->history().size();
+	return E3D_OK;
+}
+
+int e3d_history(const e3d_solver* s, int first, int count, e3d_iter_record* out) {
+	if (!s || !s->eng || !out) return fail(E3D_ERR_ARG, "null argument");
+	const auto& h = s->eng->history();
+	if (first < 0 || count < 0 || (size_t)first + (size_t)count > h.size()) return fail(E3D_ERR_ARG, "history range");
+	for (int i = 0; i < count; i++) {
+		const e3d::IterRecord& r = h[(size_t)first + i];
+		e3d_iter_record& o = out[i];
+		o.iter = r.iter;
+		for (int q = 0; q < 5; q++) {
+			o.rms[q] = r.rms[q];
+			o.conv[q] = r.conv[q];
+		}
+		o.cl = r.cl;
+		o.cd = r.cd;
+		o.cmx = r.cmx;
+		o.cmy = r.cmy;
+		o.cmz = r.cmz;
+	}
+	return E3D_OK;
+}
+
+int e3d_state_get(e3d_solver* s, int block, const char* name, double* dst, int64_t count) {
+	if (!name || !dst) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		std::vector<double> v;
+		eng(s).get(name, block, v);
+		if (count != (int64_t)v.size())
+			throw e3d::Error(E3D_ERR_ARG, std::string(name) + ": count " + std::to_string(count) + " != " +
+			                                  std::to_string(v.size()));
+		std::memcpy(dst, v.data(), v.size() * sizeof(double));
+	});
+}
+
+int e3d_state_set(e3d_solver* s, int block, const char* name, const double* src, int64_t count) {
+	if (!name || !src || count < 0) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] { eng(s).set(name, block, std::vector<double>(src, src + count)); });
+}
+
+int e3d_time_kernels(e3d_solver* s, int n_iter, char* names, int names_len, int* launches, double* total_ms,
+                     double* bytes_per_launch, int max_rows, int* rows) {
+	if (!names || !launches || !total_ms || !bytes_per_launch || !rows) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		auto t = eng(s).time_kernels(n_iter);
+		std::string joined;
+		int r = 0;
+		for (const auto& k : t) {
+			if (r >= max_rows) break;
+			if (r) joined += ",";
+			joined += k.name;
+			launches[r] = k.launches;
+			total_ms[r] = k.total_ms;
+			bytes_per_launch[r] = k.bytes_per_launch;
+			r++;
+		}
+		if ((int)joined.size() + 1 > names_len) throw e3d::Error(E3D_ERR_ARG, "names buffer too small");
+		std::memcpy(names, joined.c_str(), joined.size() + 1);
+		*rows = r;
+	});
+}
+
+int e3d_launches_per_iteration(const e3d_solver* s, int* n) {
+	if (!s || !s->eng || !n) return fail(E3D_ERR_ARG, "null argument");
+	*n = s->eng->launches_per_iteration();
+	return E3D_OK;
+}
+
+}  // extern "C"

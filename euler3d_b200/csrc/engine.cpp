@@ -1,0 +1,890 @@
+// Device-resident solver: global numbering, uploads, stage sequencing and the
+// captured outer iteration.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace e3d {
+
+namespace {
+void cuda_ok(cudaError_t e, const char* what) {
+	if (e != cudaSuccess) throw Error(E3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+}  // namespace
+
+template <class T>
+void DevBuf<T>::alloc(size_t count) {
+	free();
+	n = count;
+	if (count) cuda_ok(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+}
+template <class T>
+void DevBuf<T>::upload(const std::vector<T>& h) {
+	alloc(h.size());
+	if (!h.empty()) cuda_ok(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+}
+template <class T>
+void DevBuf<T>::free() {
+	if (p) cudaFree(p);
+	p = nullptr;
+	n = 0;
+}
+template struct DevBuf<int>;
+template struct DevBuf<signed char>;
+template struct DevBuf<double>;
+template struct DevBuf<float>;
+
+template <class T>
+FusedView<T> Engine::Fused<T>::view(bool flip) const {
+	FusedView<T> v{};
+	v.Pin = flip ? P1.p : P0.p;
+	v.Pout = flip ? P0.p : P1.p;
+	v.FS = FS.p;
+	v.Rc = Rc.p;
+	v.Rd = Rd.p;
+	v.dt = dt.p;
+	v.sgeo = sgeo.p;
+	v.sS = sS.p;
+	v.srv = srv.p;
+	v.lsw = lsw.p;
+	v.vol = vol.p;
+	return v;
+}
+
+// RK stage tables (Solver/src/RungeKutta.cpp:23-68).
+static void rk_tables(int stages, std::vector<double>& a, std::vector<double>& b) {
+	switch (stages) {
+	case 1: a = {1.0}; b = {1.0}; break;
+	case 2: a = {0.6, 1.0}; b = {1.0, 0.0}; break;
+	case 3: a = {0.6, 0.6, 1.0}; b = {1.0, 0.0, 0.0}; break;
+	case 4: a = {0.25, 1.0 / 3.0, 0.5, 1.0}; b = {1.0, 0.5, 0.0, 0.0}; break;
+	case 5: a = {0.2742, 0.2067, 0.5020, 0.5142, 1.0}; b = {1.0, 0.0, 0.56, 0.0, 0.44}; break;
+	default: throw Error(E3D_ERR_ARG, "Invalid number of RK stages: " + std::to_string(stages));
+	}
+}
+
+Engine::Engine(const HostCase& hc, const EngineOptions& opt) : deck_(hc.deck), opt_(opt) {
+	if (opt_.precision != PREC_FP64 && opt_.precision != PREC_FP32) throw Error(E3D_ERR_ARG, "unknown precision");
+	if (opt_.device >= 0) cuda_ok(cudaSetDevice(opt_.device), "cudaSetDevice");
+	carry_ = opt_.carry_w0 >= 0 ? opt_.carry_w0 : (opt_.precision == PREC_FP32 ? 1 : 0);
+	// strategy selection (ResidualCalculator.cpp:72-95, SecondOrder.cpp:50-61)
+	if (deck_.flux == "roe") scheme_ = FLUX_ROE;
+	else if (deck_.flux == "ausm") scheme_ = FLUX_AUSM;
+	else throw Error(E3D_ERR_ARG, "unknown flux scheme '" + deck_.flux + "' (roe|ausm)");
+	order_ = deck_.order == 2 ? 2 : 1;
+	grad_kind_ = deck_.gradient == "leastsquares" ? GRAD_LEAST_SQUARES : GRAD_GREEN_GAUSS;
+	lim_kind_ = deck_.limiter == "venkatakrishnan" ? LIM_VENKATAKRISHNAN : LIM_BARTH_JESPERSEN;
+	if (deck_.smoothing)
+		throw Error(E3D_ERR_ARG, "implicit residual smoothing (deck smoothing = 1) is not provided by this path");
+	rk_tables(deck_.stages, alpha_, beta_);
+	// physics constants, computed with the reference's expressions on the host
+	ph_.gamma = deck_.gamma;
+	ph_.gm1 = deck_.gamma - 1.0;
+	ph_.gr = deck_.gamma / (deck_.gamma - 1.0);
+	ph_.cfl = deck_.cfl;
+	ph_.omega = deck_.omega;
+	ph_.k3 = deck_.k * deck_.k * deck_.k;
+	{  // PrimitiveVariables::calculateFreeVariables (PrimitiveVariables.cpp:41-56)
+		const double pi = std::atan(1.0) * 4.0;
+		const double a = deck_.aoa_deg * pi / 180.0;
+		const double c = std::cos(a), s = std::sin(a);
+		ph_.free[0] = 1.0;
+		ph_.free[1] = deck_.mach * std::sqrt(deck_.gamma) * c;
+		ph_.free[2] = deck_.mach * std::sqrt(deck_.gamma) * s;
+		ph_.free[3] = 0.0;
+		ph_.free[4] = 1.0;
+	}
+	// AerodynamicParameters (AerodynamicParameters.cpp:22, :167, :212)
+	aoa_rad_ = deck_.aoa_deg * 4. * std::atan(1.) / 180;
+	denom_ = (0.5 * deck_.gamma * deck_.mach * deck_.mach) * deck_.cmac;
+
+	if (opt_.stream) {
+		st_ = opt_.stream;
+	} else {
+		cuda_ok(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
+		own_stream_ = true;
+	}
+	build(hc);
+	init_state();
+}
+
+Engine::~Engine() {
+	for (auto& g : graph_)
+		if (g) cudaGraphExecDestroy(g);
+	if (own_stream_ && st_) cudaStreamDestroy(st_);
+}
+
+void Engine::check(const char* what) { cuda_ok(cudaGetLastError(), what); }
+
+void Engine::build(const HostCase& hc) {
+	nb_ = (int)hc.blocks.size();
+	roff_.assign(nb_ + 1, 0);
+	goff_.assign(nb_ + 1, 0);
+	foff_.assign(nb_ + 1, 0);
+	for (int b = 0; b < nb_; b++) {
+		const HostBlock& B = hc.blocks[b];
+		roff_[b + 1] = roff_[b] + B.n_real;
+		goff_[b + 1] = goff_[b] + (B.n_all - B.n_real);
+		foff_[b + 1] = foff_[b] + B.n_faces;
+		n_real_b_.push_back(B.n_real);
+		n_all_b_.push_back(B.n_all);
+	}
+	NR_ = roff_[nb_];
+	NG_ = goff_[nb_];
+	NA_ = NR_ + NG_;
+	NF_ = foff_[nb_];
+	auto gid = [&](int b, int local) {
+		const HostBlock& B = hc.blocks[b];
+		return local < B.n_real ? roff_[b] + local : NR_ + goff_[b] + (local - B.n_real);
+	};
+	// slots, in global cell order
+	std::vector<int> slot_ptr(NA_ + 1, 0);
+	for (int b = 0; b < nb_; b++) {
+		const HostBlock& B = hc.blocks[b];
+		for (int c = 0; c < B.n_all; c++) slot_ptr[gid(b, c) + 1] = B.cell_face_ptr[c + 1] - B.cell_face_ptr[c];
+	}
+	for (int c = 0; c < NA_; c++) slot_ptr[c + 1] += slot_ptr[c];
+	NS_ = slot_ptr[NA_];
+	tet4_ = 1;
+	for (int c = 0; c < NR_ && tet4_; c++)
+		if (slot_ptr[c] != 4 * c || slot_ptr[c + 1] != 4 * c + 4) tet4_ = 0;
+	std::vector<int> slot_face(NS_), slot_nbr(NS_), slot_mate(NS_);
+	std::vector<double> lsw(3 * (size_t)NS_, 0.0);
+	std::vector<int> face_lr(2 * (size_t)NF_);
+	std::vector<double> S(3 * (size_t)NF_), nhat(3 * (size_t)NF_), area(NF_), rl(3 * (size_t)NF_), rr(3 * (size_t)NF_),
+	    fc(3 * (size_t)NF_), vol(NA_);
+	std::vector<int> face_slot_l(NF_, -1), face_slot_r(NF_, -1);
+	std::vector<signed char> gkind(NG_, GK_NONE), grefl(NG_, 0);
+	std::vector<int> wall_off(nb_ + 1, 0), wall_face;
+	for (int b = 0; b < nb_; b++) {
+		const HostBlock& B = hc.blocks[b];
+		for (int f = 0; f < B.n_faces; f++) {
+			const int F = foff_[b] + f;
+			face_lr[2 * (size_t)F] = gid(b, B.face_cells[2 * (size_t)f]);
+			face_lr[2 * (size_t)F + 1] = gid(b, B.face_cells[2 * (size_t)f + 1]);
+			const double a = B.face_area[f];
+			area[F] = a;
+			for (int k = 0; k < 3; k++) {
+				S[3 * (size_t)F + k] = B.face_normal[3 * (size_t)f + k];
+				// the reference normalises by the recomputed norm, which equals face_area_
+				nhat[3 * (size_t)F + k] = B.face_normal[3 * (size_t)f + k] / a;
+				rl[3 * (size_t)F + k] = B.r_left[3 * (size_t)f + k];
+				rr[3 * (size_t)F + k] = B.r_right[3 * (size_t)f + k];
+				fc[3 * (size_t)F + k] = B.face_center[3 * (size_t)f + k];
+			}
+		}
+		for (int c = 0; c < B.n_all; c++) {
+			const int g = gid(b, c);
+			vol[g] = B.cell_volume[c];
+			for (int j = B.cell_face_ptr[c]; j < B.cell_face_ptr[c + 1]; j++) {
+				const int k = slot_ptr[g] + (j - B.cell_face_ptr[c]);
+				const int F = foff_[b] + B.cell_faces[j];
+				slot_face[k] = F;
+				slot_nbr[k] = gid(b, B.cell_cells[j]);
+				if (c < B.n_real)
+					for (int d = 0; d < 3; d++) lsw[3 * (size_t)k + d] = B.ls_weights[3 * (size_t)j + d];
+				if (face_lr[2 * (size_t)F] == g) face_slot_l[F] = k;
+				else face_slot_r[F] = k;
+			}
+		}
+		for (size_t m = 0; m < B.markers.size(); m++) {
+			const Marker& mk = B.markers[m];
+			const bool real_bnd = (int)m < B.n_real_boundaries;
+			for (int gl : mk.ghosts) {
+				const int gi = gid(b, gl) - NR_;
+				grefl[gi] = real_bnd ? 1 : 0;
+				gkind[gi] = (!real_bnd || mk.kind == MK_CONNEXION) ? GK_NONE
+				            : mk.kind == MK_WALL                  ? GK_WALL
+				            : mk.kind == MK_FARFIELD              ? GK_FARFIELD
+				                                                  : GK_SYMMETRY;
+			}
+		}
+		for (int f : B.wall_faces) wall_face.push_back(foff_[b] + f);
+		wall_off[b + 1] = (int)wall_face.size();
+	}
+	for (int F = 0; F < NF_; F++)
+		if (face_slot_l[F] < 0 || face_slot_r[F] < 0) throw Error(E3D_ERR_MESH, "internal: face without two slots");
+	for (int k = 0; k < NS_; k++) {
+		const int F = slot_face[k];
+		slot_mate[k] = (face_slot_l[F] == k) ? face_slot_r[F] : ~face_slot_l[F];
+	}
+	std::vector<int> hdst, hsrc;
+	for (const Connexion& c : hc.topo.connexions)
+		for (size_t q = 0; q < c.dest_cells.size(); q++) {
+			hdst.push_back(gid(c.dest_block, c.dest_cells[q]));
+			hsrc.push_back(gid(c.origin_block, c.origin_cells[q]));
+		}
+
+	slot_ptr_.upload(slot_ptr);
+	slot_face_.upload(slot_face);
+	slot_nbr_.upload(slot_nbr);
+	slot_mate_.upload(slot_mate);
+	face_lr_.upload(face_lr);
+	halo_dst_.upload(hdst);
+	halo_src_.upload(hsrc);
+	wall_off_.upload(wall_off);
+	wall_face_.upload(wall_face);
+	roff_d_.upload(roff_);
+	gkind_.upload(gkind);
+	grefl_.upload(grefl);
+	S_.upload(S);
+	nhat_.upload(nhat);
+	area_.upload(area);
+	rl_.upload(rl);
+	rr_.upload(rr);
+	fc_.upload(fc);
+	vol64_.upload(vol);
+	lsw64_.upload(lsw);
+
+	// fused per-slot geometry, face orientation for fluxes, owner sign for GG
+	std::vector<double> sgeo(4 * (size_t)NS_), sS(3 * (size_t)NS_), srv(3 * (size_t)NS_);
+	for (int k = 0; k < NS_; k++) {
+		const int F = slot_face[k];
+		const bool left = face_slot_l[F] == k;
+		for (int d = 0; d < 3; d++) {
+			sgeo[4 * (size_t)k + d] = nhat[3 * (size_t)F + d];
+			double sv = S[3 * (size_t)F + d];
+			if (!left) sv *= -1.0;
+			sS[3 * (size_t)k + d] = sv;
+			srv[3 * (size_t)k + d] = left ? rl[3 * (size_t)F + d] : rr[3 * (size_t)F + d];
+		}
+		sgeo[4 * (size_t)k + 3] = area[F];
+	}
+	const bool need_gg = order_ == 2 && grad_kind_ == GRAD_GREEN_GAUSS;
+	const bool need_ls = order_ == 2 && grad_kind_ == GRAD_LEAST_SQUARES;
+	if (opt_.precision == PREC_FP64) {
+		f64_.sgeo.upload(sgeo);
+		if (need_gg) f64_.sS.upload(sS);
+		f64_.srv.upload(srv);
+		if (need_ls) f64_.lsw.upload(lsw);
+		f64_.vol.upload(vol);
+	} else {
+		auto tof = [](const std::vector<double>& a) { return std::vector<float>(a.begin(), a.end()); };
+		f32_.sgeo.upload(tof(sgeo));
+		if (need_gg) f32_.sS.upload(tof(sS));
+		f32_.srv.upload(tof(srv));
+		if (need_ls) f32_.lsw.upload(tof(lsw));
+		f32_.vol.upload(tof(vol));
+	}
+	// reductions: chunks of 4096 cells, never straddling a block
+	chunk_ = 4096;
+	max_chunks_ = 1;
+	for (int b = 0; b < nb_; b++) max_chunks_ = std::max(max_chunks_, (roff_[b + 1] - roff_[b] + chunk_ - 1) / chunk_);
+	partial_.alloc((size_t)nb_ * max_chunks_ * 5);
+	hist_d_.alloc(opt_.hist_capacity * (size_t)nb_ * 10);
+	fd_hist_.alloc((size_t)nb_ * 10);
+	iter_d_.alloc(1);
+	bad_d_.alloc(1);
+	zero_d_.alloc(1);
+	cuda_ok(cudaMemset(iter_d_.p, 0, sizeof(int)), "memset");
+	cuda_ok(cudaMemset(bad_d_.p, 0, sizeof(int)), "memset");
+	cuda_ok(cudaMemset(zero_d_.p, 0, sizeof(int)), "memset");
+}
+
+void Engine::init_state() {
+	// all cells, ghosts included, start at freestream
+	// (PrimitiveVariables::initializeFlowField, PrimitiveVariables.cpp:58-69);
+	// residuals, W0, gradients and limiters start at zero (value-initialised arrays)
+	std::vector<double> P(5 * (size_t)NA_);
+	for (int q = 0; q < 5; q++) std::fill(P.begin() + (size_t)q * NA_, P.begin() + (size_t)(q + 1) * NA_, ph_.free[q]);
+	std::vector<double> zR(5 * (size_t)NR_, 0.0);
+	if (opt_.precision == PREC_FP64) {
+		f64_.P0.upload(P);
+		f64_.P1.upload(P);
+		f64_.Rc.upload(zR);
+		f64_.Rd.upload(zR);
+		f64_.dt.upload(std::vector<double>(NR_, 0.0));
+		f64_.FS.alloc(order_ == 2 ? 5 * (size_t)NS_ : 0);
+		srad_.upload(std::vector<double>(NR_, 0.0));
+		grad_.upload(std::vector<double>(15 * (size_t)NA_, 0.0));
+		lim_.upload(std::vector<double>(5 * (size_t)NA_, 0.0));
+	} else {
+		std::vector<float> Pf(P.begin(), P.end());
+		f32_.P0.upload(Pf);
+		f32_.P1.upload(Pf);
+		f32_.Rc.upload(std::vector<float>(5 * (size_t)NR_, 0.f));
+		f32_.Rd.upload(std::vector<float>(5 * (size_t)NR_, 0.f));
+		f32_.dt.upload(std::vector<float>(NR_, 0.f));
+		f32_.FS.alloc(order_ == 2 ? 5 * (size_t)NS_ : 0);
+	}
+	W0_.upload(zR);
+	if (carry_) {
+		// W carried in FP64 from the freestream conservative state
+		std::vector<double> W(5 * (size_t)NR_);
+		const double* f = ph_.free;
+		for (int c = 0; c < NR_; c++) {
+			W[c] = f[0];
+			W[(size_t)NR_ + c] = f[0] * f[1];
+			W[2 * (size_t)NR_ + c] = f[0] * f[2];
+			W[3 * (size_t)NR_ + c] = f[0] * f[3];
+			W[4 * (size_t)NR_ + c] = 0.5 * f[0] * (f[1] * f[1] + f[2] * f[2] + f[3] * f[3]) + 1. / (ph_.gamma - 1.0) * f[4];
+		}
+		W0_.upload(W);
+	}
+	cur_ = 0;
+	size_t bytes = 0;
+	for (auto* b : {&slot_ptr_, &slot_face_, &slot_nbr_, &slot_mate_, &face_lr_, &halo_dst_, &halo_src_, &wall_off_,
+	                &wall_face_, &roff_d_})
+		bytes += b->n * sizeof(int);
+	for (auto* b : {&S_, &nhat_, &area_, &rl_, &rr_, &fc_, &vol64_, &lsw64_, &W0_, &srad_, &grad_, &lim_, &partial_,
+	                &hist_d_})
+		bytes += b->n * sizeof(double);
+	for (auto* b : {&f64_.P0, &f64_.P1, &f64_.FS, &f64_.Rc, &f64_.Rd, &f64_.dt, &f64_.sgeo, &f64_.sS, &f64_.srv,
+	                &f64_.lsw, &f64_.vol})
+		bytes += b->n * sizeof(double);
+	for (auto* b : {&f32_.P0, &f32_.P1, &f32_.FS, &f32_.Rc, &f32_.Rd, &f32_.dt, &f32_.sgeo, &f32_.sS, &f32_.srv,
+	                &f32_.lsw, &f32_.vol})
+		bytes += b->n * sizeof(float);
+	dev_bytes_ = bytes;
+}
+
+void Engine::require_fp64(const char* what) const {
+	if (opt_.precision != PREC_FP64)
+		throw Error(E3D_ERR_STATE, std::string(what) + " needs an FP64 solver (strategy-level calls keep the "
+		                                               "reference's FP64 arrays)");
+}
+
+StateView Engine::state64() {
+	StateView s{};
+	s.prim = cur_ ? f64_.P1.p : f64_.P0.p;
+	s.rc = f64_.Rc.p;
+	s.rd = f64_.Rd.p;
+	s.w0 = W0_.p;
+	s.grad = grad_.p;
+	s.lim = lim_.p;
+	s.dt = f64_.dt.p;
+	s.srad = srad_.p;
+	return s;
+}
+
+static GeoView make_geo(int NR, int NG, int NA, int NF, int NS, const int* sp, const int* sf, const int* sn,
+                        const int* flr, const double* S, const double* nh, const double* ar, const double* rl,
+                        const double* rr, const double* vol, const double* lsw, const signed char* gk,
+                        const signed char* gr) {
+	GeoView g{};
+	g.NR = NR;
+	g.NG = NG;
+	g.NA = NA;
+	g.NF = NF;
+	g.NS = NS;
+	g.slot_ptr = sp;
+	g.slot_face = sf;
+	g.slot_nbr = sn;
+	g.face_lr = flr;
+	g.S = S;
+	g.nhat = nh;
+	g.area = ar;
+	g.rl = rl;
+	g.rr = rr;
+	g.vol = vol;
+	g.lsw = lsw;
+	g.gkind = gk;
+	g.grefl = gr;
+	return g;
+}
+
+void Engine::block_range(int block, int& r0, int& r1, int& g0, int& g1) const {
+	if (block < -1 || block >= nb_) throw Error(E3D_ERR_ARG, "block index out of range");
+	if (block < 0) {
+		r0 = 0;
+		r1 = NR_;
+		g0 = 0;
+		g1 = NG_;
+	} else {
+		r0 = roff_[block];
+		r1 = roff_[block + 1];
+		g0 = goff_[block];
+		g1 = goff_[block + 1];
+	}
+}
+
+#define E3D_GEO                                                                                                     \
+	make_geo(NR_, NG_, NA_, NF_, NS_, slot_ptr_.p, slot_face_.p, slot_nbr_.p, face_lr_.p, S_.p, nhat_.p, area_.p, rl_.p, \
+	         rr_.p, vol64_.p, lsw64_.p, gkind_.p, grefl_.p)
+
+void Engine::save_w0(int block) {
+	require_fp64("save_w0");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	launch_save_w0(E3D_GEO, state64(), ph_, r0, r1, st_);
+	check("save_w0");
+}
+void Engine::spectral_radius(int block) {
+	require_fp64("spectral_radius");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	launch_spectral_radius(E3D_GEO, state64(), ph_, r0, r1, st_);
+	check("spectral_radius");
+}
+void Engine::timestep(int block) {
+	require_fp64("timestep");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	launch_timestep(E3D_GEO, state64(), ph_, r0, r1, st_);
+	check("timestep");
+}
+void Engine::gradients(int block, int kind) {
+	require_fp64("gradients");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	launch_gradients(E3D_GEO, state64(), kind, r0, r1, st_);
+	check("gradients");
+}
+void Engine::limiters(int block, int kind, double omega, double k) {
+	require_fp64("limiters");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	Physics ph = ph_;
+	ph.omega = omega;
+	ph.k3 = k * k * k;
+	launch_limiters(E3D_GEO, state64(), ph, kind, r0, r1, g0, g1, st_);
+	check("limiters");
+}
+void Engine::flux_conv(int block, int scheme) {
+	require_fp64("flux_conv");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	launch_flux_conv(E3D_GEO, state64(), ph_, scheme, r0, r1, st_);
+	check("flux_conv");
+}
+void Engine::flux_diss(int block, int scheme, double beta) {
+	require_fp64("flux_diss");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	launch_flux_diss(E3D_GEO, state64(), ph_, scheme, beta, r0, r1, st_);
+	check("flux_diss");
+}
+void Engine::update_internal(int block, double alpha) {
+	require_fp64("update_internal");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	launch_update(E3D_GEO, state64(), ph_, alpha, r0, r1, st_);
+	check("update_internal");
+}
+void Engine::update_boundary(int block) {
+	require_fp64("update_boundary");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	launch_bc(E3D_GEO, state64(), ph_, g0, g1, st_);
+	check("update_boundary");
+}
+void Engine::halo() {
+	if (opt_.precision == PREC_FP64)
+		launch_halo<double>((int)halo_dst_.n, halo_dst_.p, halo_src_.p, NA_, cur_ ? f64_.P1.p : f64_.P0.p,
+		                    cur_ ? f64_.P0.p : f64_.P1.p, st_);
+	else
+		launch_halo<float>((int)halo_dst_.n, halo_dst_.p, halo_src_.p, NA_, cur_ ? f32_.P1.p : f32_.P0.p,
+		                   cur_ ? f32_.P0.p : f32_.P1.p, st_);
+	check("halo");
+	started_ = true;
+}
+
+static ReduceArgs make_reduce(int NR, int NA, int nb, const int* roff, int chunk, int max_chunks, double* partial,
+                              const int* woff, const int* wface, const int* flr, const double* S, const double* fc,
+                              double denom, double* hist, const int* d_iter, int* d_bad) {
+	ReduceArgs a{};
+	a.NR = NR;
+	a.NA = NA;
+	a.nblocks = nb;
+	a.roff = roff;
+	a.chunk = chunk;
+	a.max_chunks = max_chunks;
+	a.partial = partial;
+	a.wall_off = woff;
+	a.wall_face = wface;
+	a.face_lr = flr;
+	a.S = S;
+	a.fc = fc;
+	a.denom = denom;
+	a.hist = hist;
+	a.stride = nb * 10;
+	a.d_iter = d_iter;
+	a.d_bad = d_bad;
+	return a;
+}
+
+void Engine::flow_data(std::vector<double>& out) {
+	ReduceArgs a = make_reduce(NR_, NA_, nb_, roff_d_.p, chunk_, max_chunks_, partial_.p, wall_off_.p, wall_face_.p,
+	                           face_lr_.p, S_.p, fc_.p, denom_, fd_hist_.p, zero_d_.p, bad_d_.p);
+	if (opt_.precision == PREC_FP64)
+		launch_reduce<double>(a, f64_.Rc.p, f64_.Rd.p, cur_ ? f64_.P1.p : f64_.P0.p, st_);
+	else
+		launch_reduce<float>(a, f32_.Rc.p, f32_.Rd.p, cur_ ? f32_.P1.p : f32_.P0.p, st_);
+	check("flow_data");
+	out.resize((size_t)nb_ * 10);
+	cuda_ok(cudaMemcpyAsync(out.data(), fd_hist_.p, out.size() * sizeof(double), cudaMemcpyDeviceToHost, st_), "d2h");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+}
+
+// One outer iteration (Solver::solve body, Solver.cpp:83-96, all blocks at
+// once): W0 + time step, the RK stages (RungeKutta.cpp:85-92), norms and forces
+// (PostProcessing::computeFlowData), then the inter-block halo.
+template <class T>
+void Engine::iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* marks) {
+	const int stages = (int)alpha_.size();
+	auto mark = [&]() {
+		if (marks) {
+			cudaEvent_t e;
+			cuda_ok(cudaEventCreate(&e), "event");
+			cuda_ok(cudaEventRecord(e, st_), "event");
+			marks->push_back(e);
+		}
+	};
+	int p = parity;
+	for (int s = 0; s < stages; s++) {
+		FusedView<T> v = f.view(p != 0);
+		v.NR = NR_;
+		v.NG = NG_;
+		v.NA = NA_;
+		v.NS = NS_;
+		v.tet4 = tet4_;
+		v.slot_ptr = slot_ptr_.p;
+		v.slot_nbr = slot_nbr_.p;
+		v.slot_mate = slot_mate_.p;
+		v.gkind = gkind_.p;
+		v.grefl = grefl_.p;
+		v.W0 = W0_.p;
+		if (order_ == 2) {
+			launch_recon<T>(v, ph_, grad_kind_, lim_kind_, s == 0, carry_, st_);
+			mark();
+		} else if (s == 0) {
+			launch_start<T>(v, ph_, carry_, st_);
+			mark();
+		}
+		// the reference always evaluates the dissipative flux: its guard
+		// `beta > (10^-16)` is an XOR (== -6) and is always true
+		// (ResidualCalculator.cpp:33)
+		launch_flux_update<T>(v, ph_, scheme_, order_ == 1, alpha_[s], beta_[s], s == stages - 1, carry_, st_);
+		mark();
+		p ^= 1;
+	}
+	ReduceArgs a = make_reduce(NR_, NA_, nb_, roff_d_.p, chunk_, max_chunks_, partial_.p, wall_off_.p, wall_face_.p,
+	                           face_lr_.p, S_.p, fc_.p, denom_, hist_d_.p, iter_d_.p, bad_d_.p);
+	launch_reduce<T>(a, f.Rc.p, f.Rd.p, p ? f.P1.p : f.P0.p, st_);
+	launch_halo<T>((int)halo_dst_.n, halo_dst_.p, halo_src_.p, NA_, p ? f.P1.p : f.P0.p, p ? f.P0.p : f.P1.p, st_);
+	launch_iter_advance(iter_d_.p, st_);
+	mark();
+}
+
+int Engine::launches_per_iteration() const {
+	const int stages = (int)alpha_.size();
+	return (order_ == 2 ? 2 * stages : stages + 1) + 3 /*reduce*/ + (halo_dst_.n ? 1 : 0) + 1 /*advance*/;
+}
+
+template <class T>
+void Engine::run_iterations(Fused<T>& f, int n) {
+	const int stages = (int)alpha_.size();
+	while (n > 0) {
+		const int room = (int)opt_.hist_capacity - dev_iter_;
+		const int m = std::min(n, room);
+		for (int i = 0; i < m; i++) {
+			if (opt_.use_graph) {
+				if (!graph_[cur_]) {
+					cudaGraph_t g;
+					cuda_ok(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal), "capture");
+					iteration_body<T>(f, cur_, nullptr);
+					cuda_ok(cudaStreamEndCapture(st_, &g), "capture");
+					cuda_ok(cudaGraphInstantiate(&graph_[cur_], g, 0), "graph instantiate");
+					cudaGraphDestroy(g);
+				}
+				cuda_ok(cudaGraphLaunch(graph_[cur_], st_), "graph launch");
+			} else {
+				iteration_body<T>(f, cur_, nullptr);
+				check("iteration");
+			}
+			cur_ ^= (stages & 1);
+		}
+		dev_iter_ += m;
+		n -= m;
+		collect_history(total_iter_, dev_iter_);
+	}
+}
+
+void Engine::iterate(int n) {
+	if (n < 0) throw Error(E3D_ERR_ARG, "negative iteration count");
+	if (!started_) halo();  // Solver.cpp:48, before the first iteration
+	if (opt_.precision == PREC_FP64) run_iterations(f64_, n);
+	else run_iterations(f32_, n);
+}
+
+// Pulls the device history records, converts them to the reference's mesh-level
+// quantities, and resets the device counter.
+void Engine::collect_history(int first_iter, int n) {
+	if (n <= 0) return;
+	std::vector<double> h((size_t)n * nb_ * 10);
+	cuda_ok(cudaMemcpyAsync(h.data(), hist_d_.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st_), "d2h");
+	cuda_ok(cudaMemsetAsync(iter_d_.p, 0, sizeof(int), st_), "memset");
+	int bad = 0;
+	cuda_ok(cudaMemcpyAsync(&bad, bad_d_.p, sizeof(int), cudaMemcpyDeviceToHost, st_), "d2h");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	dev_iter_ = 0;
+	for (int i = 0; i < n; i++) {
+		IterRecord r{};
+		r.iter = first_iter + i;
+		for (int b = 0; b < nb_; b++) {
+			const double* x = &h[((size_t)i * nb_ + b) * 10];
+			const double N = (double)(roff_[b + 1] - roff_[b]);
+			// Convergence::calculate*Rms (Convergence.cpp:27-48) then the block sum
+			// (BlockCommunicator.cpp:342-369)
+			for (int q = 0; q < 5; q++) r.rms[q] += (1. / N) * std::pow(x[q], 0.5);
+			// AerodynamicParameters::calculateGlobalCl/Cd (AerodynamicParameters.cpp:114-138)
+			const double cl_ = x[5], cd_ = x[6];
+			r.cl += cl_ * std::cos(aoa_rad_) - cd_ * std::sin(aoa_rad_);
+			r.cd += cl_ * std::sin(aoa_rad_) + cd_ * std::cos(aoa_rad_);
+			r.cmx += x[7];
+			r.cmy += x[8];
+			r.cmz += x[9];
+		}
+		if (!have_rms0_) {
+			for (int q = 0; q < 5; q++) rms0_[q] = r.rms[q];
+			have_rms0_ = true;
+		}
+		for (int q = 0; q < 5; q++) r.conv[q] = std::log10(r.rms[q]) - std::log10(rms0_[q]);
+		hist_.push_back(r);
+	}
+	total_iter_ += n;
+	if (bad) throw Error(E3D_ERR_NONFINITE, "non-finite residual norm by iteration " + std::to_string(total_iter_ - 1));
+}
+
+int Engine::solve(int max_iter, double criterion, int check_every) {
+	if (check_every < 1) check_every = 1;
+	int done = 0;
+	while (true) {
+		const size_t before = hist_.size();
+		iterate(std::min(check_every, std::max(1, max_iter - total_iter_)));
+		for (size_t i = before; i < hist_.size(); i++) {
+			// PostProcessing::checkStopSolver (PostProcessing.cpp:77)
+			if (hist_[i].iter + 1 == max_iter || hist_[i].conv[0] <= criterion) return hist_[i].iter + 1;
+		}
+		done = total_iter_;
+		if (done >= max_iter) return done;
+	}
+}
+
+void Engine::sync() {
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	int bad = 0;
+	cuda_ok(cudaMemcpy(&bad, bad_d_.p, sizeof(int), cudaMemcpyDeviceToHost), "d2h");
+	if (bad) throw Error(E3D_ERR_NONFINITE, "non-finite residual norm");
+}
+
+// ---------------------------------------------------------------- state transfer
+namespace {
+template <class T>
+void d2h_rows(const T* dev, int ld, int rows, int begin, int count, std::vector<double>& out, size_t out_off,
+              int out_ld, cudaStream_t st) {
+	std::vector<T> tmp((size_t)count);
+	for (int q = 0; q < rows; q++) {
+		if (count == 0) continue;
+		cuda_ok(cudaMemcpyAsync(tmp.data(), dev + (size_t)q * ld + begin, count * sizeof(T), cudaMemcpyDeviceToHost, st),
+		        "d2h");
+		cuda_ok(cudaStreamSynchronize(st), "sync");
+		for (int i = 0; i < count; i++) out[out_off + (size_t)q * out_ld + i] = (double)tmp[i];
+	}
+}
+template <class T>
+void h2d_rows(T* dev, int ld, int rows, int begin, int count, const std::vector<double>& in, size_t in_off, int in_ld,
+              cudaStream_t st) {
+	std::vector<T> tmp((size_t)count);
+	for (int q = 0; q < rows; q++) {
+		if (count == 0) continue;
+		for (int i = 0; i < count; i++) tmp[i] = (T)in[in_off + (size_t)q * in_ld + i];
+		cuda_ok(cudaMemcpyAsync(dev + (size_t)q * ld + begin, tmp.data(), count * sizeof(T), cudaMemcpyHostToDevice, st),
+		        "h2d");
+		cuda_ok(cudaStreamSynchronize(st), "sync");
+	}
+}
+}  // namespace
+
+// Names and layouts match the reference's arrays for block `block`:
+//   prim [5][n_all], limiter [5][n_all], grad [5][n_all][3],
+//   conv_res/diss_res/w0 [5][n_real], dt/spectral_radius [n_real]
+void Engine::get(const std::string& name, int b, std::vector<double>& out) {
+	if (b < 0 || b >= nb_) throw Error(E3D_ERR_ARG, "block index out of range");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	const int nr = n_real_b_[b], na = n_all_b_[b], ng = na - nr, r0 = roff_[b], g0 = NR_ + goff_[b];
+	const bool f64 = opt_.precision == PREC_FP64;
+	auto rows_all = [&](int rows, auto* dev) {
+		out.assign((size_t)rows * na, 0.0);
+		d2h_rows(dev, NA_, rows, r0, nr, out, 0, na, st_);
+		d2h_rows(dev, NA_, rows, g0, ng, out, nr, na, st_);
+	};
+	auto rows_real = [&](int rows, auto* dev) {
+		out.assign((size_t)rows * nr, 0.0);
+		d2h_rows(dev, NR_, rows, r0, nr, out, 0, nr, st_);
+	};
+	if (name == "prim") {
+		if (f64) rows_all(5, cur_ ? f64_.P1.p : f64_.P0.p);
+		else rows_all(5, cur_ ? f32_.P1.p : f32_.P0.p);
+	} else if (name == "conv_res") {
+		if (f64) rows_real(5, f64_.Rc.p);
+		else rows_real(5, f32_.Rc.p);
+	} else if (name == "diss_res") {
+		if (f64) rows_real(5, f64_.Rd.p);
+		else rows_real(5, f32_.Rd.p);
+	} else if (name == "w0") {
+		rows_real(5, W0_.p);
+	} else if (name == "dt") {
+		if (f64) rows_real(1, f64_.dt.p);
+		else rows_real(1, f32_.dt.p);
+	} else if (name == "spectral_radius") {
+		require_fp64("spectral_radius download");
+		rows_real(1, srad_.p);
+	} else if (name == "limiter") {
+		require_fp64("limiter download");
+		rows_all(5, lim_.p);
+	} else if (name == "grad") {
+		require_fp64("grad download");
+		std::vector<double> t;
+		out.swap(t);
+		rows_all(15, grad_.p);  // [var*3+dim][cell]
+		std::vector<double> o((size_t)15 * na);
+		for (int q = 0; q < 5; q++)
+			for (int c = 0; c < na; c++)
+				for (int d = 0; d < 3; d++) o[((size_t)q * na + c) * 3 + d] = out[(size_t)(q * 3 + d) * na + c];
+		out.swap(o);
+	} else {
+		throw Error(E3D_ERR_ARG, "unknown state array '" + name + "'");
+	}
+}
+
+void Engine::set(const std::string& name, int b, const std::vector<double>& in) {
+	if (b < 0 || b >= nb_) throw Error(E3D_ERR_ARG, "block index out of range");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	const int nr = n_real_b_[b], na = n_all_b_[b], ng = na - nr, r0 = roff_[b], g0 = NR_ + goff_[b];
+	const bool f64 = opt_.precision == PREC_FP64;
+	auto put_all = [&](int rows, auto* dev) {
+		if (in.size() != (size_t)rows * na) throw Error(E3D_ERR_ARG, name + ": wrong length");
+		h2d_rows(dev, NA_, rows, r0, nr, in, 0, na, st_);
+		h2d_rows(dev, NA_, rows, g0, ng, in, nr, na, st_);
+	};
+	auto put_real = [&](int rows, auto* dev) {
+		if (in.size() != (size_t)rows * nr) throw Error(E3D_ERR_ARG, name + ": wrong length");
+		h2d_rows(dev, NR_, rows, r0, nr, in, 0, nr, st_);
+	};
+	if (name == "prim") {
+		// both ping-pong buffers, so ghost cells that no stage rewrites stay consistent
+		if (f64) {
+			put_all(5, f64_.P0.p);
+			put_all(5, f64_.P1.p);
+		} else {
+			put_all(5, f32_.P0.p);
+			put_all(5, f32_.P1.p);
+		}
+	} else if (name == "conv_res") {
+		if (f64) put_real(5, f64_.Rc.p);
+		else put_real(5, f32_.Rc.p);
+	} else if (name == "diss_res") {
+		if (f64) put_real(5, f64_.Rd.p);
+		else put_real(5, f32_.Rd.p);
+	} else if (name == "w0") {
+		put_real(5, W0_.p);
+	} else if (name == "dt") {
+		if (f64) put_real(1, f64_.dt.p);
+		else put_real(1, f32_.dt.p);
+	} else if (name == "limiter") {
+		require_fp64("limiter upload");
+		put_all(5, lim_.p);
+	} else if (name == "grad") {
+		require_fp64("grad upload");
+		if (in.size() != (size_t)15 * na) throw Error(E3D_ERR_ARG, "grad: wrong length");
+		std::vector<double> t((size_t)15 * na);
+		for (int q = 0; q < 5; q++)
+			for (int c = 0; c < na; c++)
+				for (int d = 0; d < 3; d++) t[(size_t)(q * 3 + d) * na + c] = in[((size_t)q * na + c) * 3 + d];
+		h2d_rows(grad_.p, NA_, 15, r0, nr, t, 0, na, st_);
+		h2d_rows(grad_.p, NA_, 15, g0, ng, t, nr, na, st_);
+	} else {
+		throw Error(E3D_ERR_ARG, "unknown or read-only state array '" + name + "'");
+	}
+}
+
+// ---------------------------------------------------------------- measurement
+double Engine::bytes_recon(bool first) const {
+	const double b = opt_.precision == PREC_FP64 ? 8.0 : 4.0;
+	const double NSR = tet4_ ? 4.0 * NR_ : (double)NS_ - NG_;
+	double x = 5 * b * NA_                                  // cell states, every cell read once
+	           + 4.0 * NSR + 4.0 * NG_                      // neighbour ids (+ ghost mates)
+	           + 3 * b * NSR                                // LS weights or signed area vectors
+	           + 3 * b * NS_                                // r-vectors, ghost slots included
+	           + b * NA_                                    // volumes
+	           + 4 * b * NG_ + 2.0 * NG_                    // ghost face normals, ghost flags
+	           + 5 * b * NS_;                               // face states written
+	if (first) x += 5 * 8.0 * (carry_ ? 0 : NR_) + b * NR_ + 4 * b * NSR;  // W0, dt written; face normals
+	return x;
+}
+double Engine::bytes_start() const {
+	const double b = opt_.precision == PREC_FP64 ? 8.0 : 4.0;
+	const double NSR = tet4_ ? 4.0 * NR_ : (double)NS_ - NG_;
+	return 5 * b * NR_ + 4 * b * NSR + b * NR_ + 5 * 8.0 * (carry_ ? 0 : NR_) + b * NR_;
+}
+double Engine::bytes_flux(bool order1) const {
+	const double b = opt_.precision == PREC_FP64 ? 8.0 : 4.0;
+	const double NSR = tet4_ ? 4.0 * NR_ : (double)NS_ - NG_;
+	double x = 4.0 * NSR + 4.0 * NSR       // mate and neighbour ids
+	           + 4 * b * NSR               // face normal and area
+	           + 5 * b * NR_ * 2           // Rd read, Rc written
+	           + 5 * b * NR_               // Rd written
+	           + 5 * 8.0 * NR_             // W0 read
+	           + 2 * b * NR_               // dt, volume
+	           + 5 * b * NA_               // new cell and ghost states written
+	           + 1.0 * NG_;                // ghost kinds
+	x += order1 ? 5 * b * NA_ : 5 * b * NS_;  // cell states or face states read
+	return x;
+}
+
+std::vector<Engine::KernelTime> Engine::time_kernels(int n) {
+	std::vector<KernelTime> out;
+	if (!started_) halo();
+	const int stages = (int)alpha_.size();
+	std::vector<std::string> names;
+	std::vector<double> bytes;
+	for (int s = 0; s < stages; s++) {
+		if (order_ == 2) {
+			names.push_back(s == 0 ? "recon_first" : "recon");
+			bytes.push_back(bytes_recon(s == 0));
+		} else if (s == 0) {
+			names.push_back("start");
+			bytes.push_back(bytes_start());
+		}
+		names.push_back("flux_update");
+		bytes.push_back(bytes_flux(order_ == 1));
+	}
+	names.push_back("reduce_halo");
+	bytes.push_back(0.0);
+	std::vector<double> acc(names.size(), 0.0);
+	for (int it = 0; it < n; it++) {
+		std::vector<cudaEvent_t> marks;
+		cudaEvent_t e0;
+		cuda_ok(cudaEventCreate(&e0), "event");
+		cuda_ok(cudaEventRecord(e0, st_), "event");
+		marks.push_back(e0);
+		if (opt_.precision == PREC_FP64) iteration_body<double>(f64_, cur_, &marks);
+		else iteration_body<float>(f32_, cur_, &marks);
+		cur_ ^= (stages & 1);
+		cuda_ok(cudaEventSynchronize(marks.back()), "event sync");
+		for (size_t i = 1; i < marks.size() && i - 1 < acc.size(); i++) {
+			float ms = 0.f;
+			cuda_ok(cudaEventElapsedTime(&ms, marks[i - 1], marks[i]), "elapsed");
+			acc[i - 1] += ms;
+		}
+		for (auto e : marks) cudaEventDestroy(e);
+		dev_iter_ += 1;
+		if (dev_iter_ >= (int)opt_.hist_capacity) collect_history(total_iter_, dev_iter_);
+	}
+	collect_history(total_iter_, dev_iter_);
+	// merge repeated names
+	for (size_t i = 0; i < names.size(); i++) {
+		auto it = std::find_if(out.begin(), out.end(), [&](const KernelTime& k) { return k.name == names[i]; });
+		if (it == out.end()) out.push_back({names[i], n, acc[i], bytes[i]});
+		else {
+			it->launches += n;
+			it->total_ms += acc[i];
+		}
+	}
+	return out;
+}
+
+}  // namespace e3d

@@ -1,0 +1,154 @@
+// Device-resident solver over one case (all blocks on one GPU).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "launch.hpp"
+#include "mesh.hpp"
+
+namespace e3d {
+
+enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1 };
+
+struct EngineOptions {
+	int precision = PREC_FP64;
+	int carry_w0 = -1;   // -1: default (off for FP64, on for FP32): keep W in FP64 across iterations
+	int use_graph = 1;   // capture one outer iteration in a CUDA graph
+	int device = -1;     // -1: current device
+	cudaStream_t stream = nullptr;  // nullptr: the engine creates its own stream
+	size_t hist_capacity = 4096;    // iterations of per-block norm/force history kept on device
+};
+
+// Host copy of one outer iteration's results (reference PostProcessing fields).
+struct IterRecord {
+	int iter;
+	double rms[5];          // mesh residual norms (sum of per-block norms)
+	double conv[5];         // log10(rms) - log10(rms at iteration 0)
+	double cl, cd, cmx, cmy, cmz;
+};
+
+template <class T>
+struct DevBuf {
+	T* p = nullptr;
+	size_t n = 0;
+	void alloc(size_t count);
+	void upload(const std::vector<T>& h);
+	void free();
+	~DevBuf() { free(); }
+};
+
+class Engine {
+public:
+	Engine(const HostCase& hc, const EngineOptions& opt);
+	~Engine();
+	Engine(const Engine&) = delete;
+	Engine& operator=(const Engine&) = delete;
+
+	// --- strategy-level operations (FP64 engine); block = -1 means every block
+	void save_w0(int block);
+	void spectral_radius(int block);
+	void timestep(int block);
+	void gradients(int block, int kind);
+	void limiters(int block, int kind, double omega, double k);
+	void flux_conv(int block, int scheme);
+	void flux_diss(int block, int scheme, double beta);
+	void update_internal(int block, double alpha);
+	void update_boundary(int block);
+	void halo();
+	// per-block norms and forces of the current state (PostProcessing::computeFlowData)
+	void flow_data(std::vector<double>& per_block10);
+
+	// --- whole outer iterations (fused kernels); appends to history()
+	void iterate(int n_iter);
+	// run until the reference stop test (max_iter or criterion) fires
+	int solve(int max_iter, double criterion, int check_every);
+
+	const std::vector<IterRecord>& history() const { return hist_; }
+	void sync();  // waits for queued work; throws on a CUDA error or a non-finite norm
+
+	// --- state transfer (block-local cell order, FP64 on the host side)
+	void get(const std::string& name, int block, std::vector<double>& out);
+	void set(const std::string& name, int block, const std::vector<double>& in);
+
+	int n_blocks() const { return nb_; }
+	int n_real(int b) const { return roff_[b + 1] - roff_[b]; }
+	long long n_real_total() const { return NR_; }
+	int precision() const { return opt_.precision; }
+	cudaStream_t stream() const { return st_; }
+	size_t device_bytes() const { return dev_bytes_; }
+	// number of kernel launches one outer iteration issues
+	int launches_per_iteration() const;
+	const Deck& deck() const { return deck_; }
+	// algorithmic bytes (distinct elements touched) of one launch of each fused kernel
+	double bytes_recon(bool first) const;
+	double bytes_start() const;
+	double bytes_flux(bool order1) const;
+	// times each fused kernel of `n` eager (un-captured) iterations with CUDA events on
+	// the engine stream; returns {name, launches, total_ms}
+	struct KernelTime {
+		std::string name;
+		int launches;
+		double total_ms;
+		double bytes_per_launch;
+	};
+	std::vector<KernelTime> time_kernels(int n);
+
+private:
+	template <class T>
+	struct Fused {
+		DevBuf<T> P0, P1, FS, Rc, Rd, dt, sgeo, sS, srv, lsw, vol;
+		FusedView<T> view(bool flip) const;
+	};
+	void build(const HostCase& hc);
+	void init_state();
+	void check(const char* what);
+	template <class T>
+	void iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* marks);
+	template <class T>
+	void run_iterations(Fused<T>& f, int n);
+	void collect_history(int first_iter, int n);
+	void block_range(int block, int& r0, int& r1, int& g0, int& g1) const;
+	void require_fp64(const char* what) const;
+	StateView state64();
+	const double* cur_prim64() const;
+
+	Deck deck_;
+	EngineOptions opt_;
+	cudaStream_t st_ = nullptr;
+	bool own_stream_ = false;
+	int nb_ = 0, NR_ = 0, NG_ = 0, NA_ = 0, NF_ = 0, NS_ = 0, tet4_ = 0;
+	std::vector<int> roff_, goff_, foff_, soff_;  // per block offsets (nb_+1)
+	std::vector<int> n_real_b_, n_all_b_;
+	Physics ph_{};
+	double denom_ = 1.0, aoa_rad_ = 0.0;
+	int carry_ = 0;
+	int grad_kind_ = GRAD_LEAST_SQUARES, lim_kind_ = LIM_VENKATAKRISHNAN, scheme_ = FLUX_ROE, order_ = 1;
+	std::vector<double> alpha_, beta_;
+	// geometry / topology
+	DevBuf<int> slot_ptr_, slot_face_, slot_nbr_, slot_mate_, face_lr_, halo_dst_, halo_src_, wall_off_, wall_face_,
+	    roff_d_;
+	DevBuf<signed char> gkind_, grefl_;
+	DevBuf<double> S_, nhat_, area_, rl_, rr_, fc_, vol64_, lsw64_;
+	// FP64 strategy-level state
+	DevBuf<double> W0_, srad_, grad_, lim_;
+	Fused<double> f64_;
+	Fused<float> f32_;
+	int cur_ = 0;  // which of P0/P1 holds the current state
+	// reductions
+	DevBuf<double> partial_, hist_d_, fd_hist_;
+	DevBuf<int> iter_d_, bad_d_, zero_d_;
+	bool started_ = false;
+	int chunk_ = 0, max_chunks_ = 0;
+	int dev_iter_ = 0;  // iterations recorded on the device since the last collect
+	int total_iter_ = 0;
+	bool have_rms0_ = false;
+	double rms0_[5] = {0, 0, 0, 0, 0};
+	std::vector<IterRecord> hist_;
+	cudaGraphExec_t graph_[2] = {nullptr, nullptr};
+	size_t dev_bytes_ = 0;
+};
+
+}  // namespace e3d

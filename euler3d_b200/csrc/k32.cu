@@ -1,0 +1,13 @@
+// FP32 instantiations of the fused path (multiply-add contraction allowed).
+#include "launch_common.cuh"
+
+namespace e3d {
+
+template void launch_halo<float>(int, const int*, const int*, int, float*, float*, cudaStream_t);
+template void launch_reduce<float>(const ReduceArgs&, const float*, const float*, const float*, cudaStream_t);
+template void launch_recon<float>(const FusedView<float>&, const Physics&, int, int, bool, int, cudaStream_t);
+template void launch_start<float>(const FusedView<float>&, const Physics&, int, cudaStream_t);
+template void launch_flux_update<float>(const FusedView<float>&, const Physics&, int, bool, double, double, int, int,
+                                        cudaStream_t);
+
+}  // namespace e3d

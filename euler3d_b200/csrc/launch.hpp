@@ -1,0 +1,59 @@
+// Host-callable kernel launchers.  k64.cu (built with -fmad=false, so double
+// arithmetic keeps the reference's rounding) defines the FP64 granular kernels
+// and the double instantiations; k32.cu defines the float instantiations.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "views.hpp"
+
+namespace e3d {
+
+// ---- granular FP64 drop-in kernels (one per reference strategy method) ----
+void launch_save_w0(const GeoView&, const StateView&, const Physics&, int r0, int r1, cudaStream_t);
+void launch_spectral_radius(const GeoView&, const StateView&, const Physics&, int r0, int r1, cudaStream_t);
+void launch_timestep(const GeoView&, const StateView&, const Physics&, int r0, int r1, cudaStream_t);
+void launch_gradients(const GeoView&, const StateView&, int kind, int r0, int r1, cudaStream_t);
+void launch_limiters(const GeoView&, const StateView&, const Physics&, int kind, int r0, int r1, int g0, int g1,
+                     cudaStream_t);
+void launch_flux_conv(const GeoView&, const StateView&, const Physics&, int scheme, int r0, int r1, cudaStream_t);
+void launch_flux_diss(const GeoView&, const StateView&, const Physics&, int scheme, double beta, int r0, int r1,
+                      cudaStream_t);
+void launch_update(const GeoView&, const StateView&, const Physics&, double alpha, int r0, int r1, cudaStream_t);
+void launch_bc(const GeoView&, const StateView&, const Physics&, int g0, int g1, cudaStream_t);
+
+// ---- shared by both paths, per precision ----
+template <class T>
+void launch_halo(int n, const int* dst, const int* src, int NA, T* b0, T* b1, cudaStream_t);
+
+// Per-block reductions written into hist[iter*stride + b*10 + (0..4 norms, 5..9 forces)],
+// iter read from *d_iter (the device iteration counter).
+struct ReduceArgs {
+	int NR, NA, nblocks;
+	const int* roff;       // nblocks+1 real-cell offsets
+	int chunk, max_chunks;
+	double* partial;       // nblocks*max_chunks*5
+	const int* wall_off;   // nblocks+1
+	const int* wall_face;
+	const int* face_lr;
+	const double* S;
+	const double* fc;
+	double denom;          // 0.5*gamma*M*M*cmac
+	double* hist;
+	int stride;
+	const int* d_iter;
+	int* d_bad;
+};
+template <class T>
+void launch_reduce(const ReduceArgs&, const T* Rc, const T* Rd, const T* P, cudaStream_t);
+void launch_iter_advance(int* d_iter, cudaStream_t);
+
+// ---- fused stage kernels ----
+template <class T>
+void launch_recon(const FusedView<T>&, const Physics&, int grad, int lim, bool first, int carry, cudaStream_t);
+template <class T>
+void launch_start(const FusedView<T>&, const Physics&, int carry, cudaStream_t);
+template <class T>
+void launch_flux_update(const FusedView<T>&, const Physics&, int scheme, bool order1, double alpha, double beta,
+                        int last, int carry, cudaStream_t);
+
+}  // namespace e3d

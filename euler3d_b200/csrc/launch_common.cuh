@@ -1,0 +1,67 @@
+// Launcher templates shared by k64.cu and k32.cu (each instantiates its T).
+#pragma once
+#include "kernels.cuh"
+#include "launch.hpp"
+
+namespace e3d {
+
+template <class T>
+void launch_halo(int n, const int* dst, const int* src, int NA, T* b0, T* b1, cudaStream_t st) {
+	if (n > 0) k_halo<T><<<(n + 127) / 128, 128, 0, st>>>(n, dst, src, NA, b0, b1);
+}
+
+template <class T>
+void launch_reduce(const ReduceArgs& a, const T* Rc, const T* Rd, const T* P, cudaStream_t st) {
+	constexpr int THREADS = 256;
+	dim3 grid(a.max_chunks, a.nblocks);
+	k_norm_partial<T, THREADS><<<grid, THREADS, 0, st>>>(Rc, Rd, a.NR, a.roff, a.chunk, a.max_chunks, a.partial);
+	k_norm_final<<<(a.nblocks * 5 + 127) / 128, 128, 0, st>>>(a.partial, a.nblocks, a.max_chunks, a.hist, a.stride,
+	                                                         a.d_iter, a.d_bad);
+	k_forces<T><<<(a.nblocks + 63) / 64, 64, 0, st>>>(P, a.NA, a.wall_off, a.wall_face, a.face_lr, a.S, a.fc, a.denom,
+	                                                  a.nblocks, a.hist, a.stride, a.d_iter);
+}
+
+template <class T, int GRAD, int LIM>
+void recon_dispatch_first(const FusedView<T>& v, const Physics& ph, bool first, int carry, cudaStream_t st) {
+	const int grid = (v.NR + 127) / 128;
+	if (first) k_recon<T, GRAD, LIM, true><<<grid, 128, 0, st>>>(v, ph, carry);
+	else k_recon<T, GRAD, LIM, false><<<grid, 128, 0, st>>>(v, ph, carry);
+}
+
+template <class T>
+void launch_recon(const FusedView<T>& v, const Physics& ph, int grad, int lim, bool first, int carry, cudaStream_t st) {
+	if (v.NR <= 0) return;
+	if (grad == GRAD_LEAST_SQUARES) {
+		if (lim == LIM_VENKATAKRISHNAN)
+			recon_dispatch_first<T, GRAD_LEAST_SQUARES, LIM_VENKATAKRISHNAN>(v, ph, first, carry, st);
+		else
+			recon_dispatch_first<T, GRAD_LEAST_SQUARES, LIM_BARTH_JESPERSEN>(v, ph, first, carry, st);
+	} else {
+		if (lim == LIM_VENKATAKRISHNAN)
+			recon_dispatch_first<T, GRAD_GREEN_GAUSS, LIM_VENKATAKRISHNAN>(v, ph, first, carry, st);
+		else
+			recon_dispatch_first<T, GRAD_GREEN_GAUSS, LIM_BARTH_JESPERSEN>(v, ph, first, carry, st);
+	}
+}
+
+template <class T>
+void launch_start(const FusedView<T>& v, const Physics& ph, int carry, cudaStream_t st) {
+	if (v.NR > 0) k_start<T><<<(v.NR + 127) / 128, 128, 0, st>>>(v, ph, carry);
+}
+
+template <class T>
+void launch_flux_update(const FusedView<T>& v, const Physics& ph, int scheme, bool order1, double alpha, double beta,
+                        int last, int carry, cudaStream_t st) {
+	if (v.NR <= 0) return;
+	const int grid = (v.NR + 127) / 128;
+	const T a = T(alpha), b = T(beta);
+	if (scheme == FLUX_AUSM) {
+		if (order1) k_flux_update<T, FLUX_AUSM, true><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);
+		else k_flux_update<T, FLUX_AUSM, false><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);
+	} else {
+		if (order1) k_flux_update<T, FLUX_ROE, true><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);
+		else k_flux_update<T, FLUX_ROE, false><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);
+	}
+}
+
+}  // namespace e3d

@@ -288,6 +288,69 @@ def write_deck(path: str, d: Deck) -> None:
         f.write(txt)
 
 
+def hex_channel(n: int, nz: int = 1, height: float = 0.05, sigma: float = 0.1) -> BlockMesh:
+    """A 2.5-D hexahedron channel: n x n x nz hexes (SU2 type 12), WALL at y=0,
+    SYMMETRY at z=0 and z=1, FARFIELD elsewhere.  Exercises quadrilateral
+    faces and symmetry ghosts (the reference's NACA test mesh has the same
+    marker mix)."""
+    m = n + 1
+    ii, jj, kk = np.meshgrid(np.arange(m), np.arange(m), np.arange(nz + 1), indexing="ij")
+    ijk = np.stack([ii.transpose(2, 1, 0).ravel(), jj.transpose(2, 1, 0).ravel(),
+                    kk.transpose(2, 1, 0).ravel()], axis=1).astype(np.int64)
+    x = ijk[:, 0] / n
+    y = ijk[:, 1] / n
+    z = ijk[:, 2] / nz
+    h = height * np.exp(-((x - 0.5) ** 2) / (2.0 * sigma * sigma))
+    nodes = np.stack([x, y + h * (1.0 - y), z], axis=1)
+
+    def nid(i, j, k):
+        return i + m * (j + m * k)
+
+    hi, hj, hk = np.meshgrid(np.arange(n), np.arange(n), np.arange(nz), indexing="ij")
+    hi, hj, hk = (a.transpose(2, 1, 0).ravel() for a in (hi, hj, hk))
+    # SU2 hexahedron order: bottom quad (z-) counter-clockwise, then top quad
+    hexes = np.stack([nid(hi, hj, hk), nid(hi + 1, hj, hk), nid(hi + 1, hj + 1, hk), nid(hi, hj + 1, hk),
+                      nid(hi, hj, hk + 1), nid(hi + 1, hj, hk + 1), nid(hi + 1, hj + 1, hk + 1),
+                      nid(hi, hj + 1, hk + 1)], axis=1)
+    wall = [(nid(i, 0, k), nid(i + 1, 0, k), nid(i + 1, 0, k + 1), nid(i, 0, k + 1))
+            for k in range(nz) for i in range(n)]
+    sym = [(nid(i, j, kz), nid(i + 1, j, kz), nid(i + 1, j + 1, kz), nid(i, j + 1, kz))
+           for kz in (0, nz) for j in range(n) for i in range(n)]
+    far = [(nid(i, n, k), nid(i + 1, n, k), nid(i + 1, n, k + 1), nid(i, n, k + 1)) for k in range(nz) for i in range(n)]
+    far += [(nid(ie, j, k), nid(ie, j + 1, k), nid(ie, j + 1, k + 1), nid(ie, j, k + 1))
+            for ie in (0, n) for k in range(nz) for j in range(n)]
+    blk = BlockMesh(nodes=nodes, tets=hexes)
+    blk.markers = [("WALL", np.array(wall)), ("SYMMETRY", np.array(sym)), ("FARFIELD", np.array(far))]
+    return blk
+
+
+def write_su2_hex(path: str, blk: BlockMesh) -> None:
+    """Like write_su2 for hexahedra (type 12) with quadrilateral markers (type 9)."""
+    parts = ["NDIME= 3\n", "\n", f"NPOIN= {blk.nodes.shape[0]}\n", _fmt_coords(blk.nodes), "\n",
+             f"NELEM= {blk.tets.shape[0]}\n", _fast_int_rows("12 ", blk.tets), "\n",
+             f"NMARK= {len(blk.markers)}\n"]
+    for tag, faces in blk.markers:
+        parts.append(f"MARKER_TAG= {tag}\n")
+        parts.append(f"MARKER_ELEMS= {faces.shape[0]}\n")
+        parts.append(_fast_int_rows("9 ", faces) if faces.shape[0] else "")
+    with open(path, "w") as f:
+        f.write("".join(parts))
+
+
+def write_hex_case(directory: str, n: int, nz: int = 1, prefix: str = "hexchan", deck: Deck | None = None) -> str:
+    """Single-block hexahedron channel case; returns the deck path."""
+    os.makedirs(directory, exist_ok=True)
+    blk = hex_channel(n, nz)
+    write_su2_hex(os.path.join(directory, prefix + ".su2"), blk)
+    write_topology(os.path.join(directory, prefix + ".top"), [prefix + ".su2"], [blk])
+    d = deck or Deck(topology=prefix + ".top")
+    d.topology = prefix + ".top"
+    deck_path = os.path.join(directory, prefix + ".deck")
+    write_deck(deck_path, d)
+    os.makedirs(os.path.join(directory, "bin"), exist_ok=True)
+    return deck_path
+
+
 def write_case(directory: str, n: int, n_blocks: int = 1, prefix: str = "bump",
                deck: Deck | None = None, height: float = 0.05, sigma: float = 0.1) -> str:
     """Generate a bump-channel case in ``directory``; return the deck path.

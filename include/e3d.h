@@ -1,0 +1,158 @@
+/*
+ * e3d.h -- C ABI of the B200 residual-and-update path for euler3D cases.
+ *
+ * Plain C types only (no CUDA, no torch, no C++ in the signatures).  Every
+ * function returns an int status: 0 on success, a negative E3D_ERR_* code on
+ * failure, with a message available from e3d_last_error() on the calling
+ * thread.  Nothing here calls exit() or traps on the device.
+ *
+ * Each entry point names the reference interface it replaces (file:line in
+ * guillaumetousignant/euler3D).  A "block" argument of -1 applies the call to
+ * every block, which is what one outer iteration of the reference does block
+ * after block (Solver/src/Solver.cpp:83-91).
+ */
+#ifndef E3D_H
+#define E3D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define E3D_OK 0
+#define E3D_ERR_ARG (-1)       /* bad argument or unsupported deck option */
+#define E3D_ERR_IO (-2)        /* file cannot be opened or read */
+#define E3D_ERR_FORMAT (-3)    /* deck / topology / SU2 syntax */
+#define E3D_ERR_MESH (-4)      /* inconsistent mesh (open cell, face shared by 3 cells, ...) */
+#define E3D_ERR_CUDA (-5)      /* CUDA runtime error */
+#define E3D_ERR_NONFINITE (-6) /* a residual norm became NaN or infinite */
+#define E3D_ERR_STATE (-7)     /* call not valid in this solver state / precision */
+#define E3D_ERR_TIMEOUT (-8)   /* a bounded wait expired */
+#define E3D_ERR_LIMIT (-9)     /* size above a documented maximum */
+
+/* strategy selectors: the reference's string choices
+ * (ResidualCalculator.cpp:72-95, SecondOrder.cpp:50-61) */
+#define E3D_GRAD_GREEN_GAUSS 0
+#define E3D_GRAD_LEAST_SQUARES 1
+#define E3D_LIM_BARTH_JESPERSEN 0
+#define E3D_LIM_VENKATAKRISHNAN 1
+#define E3D_FLUX_ROE 0
+#define E3D_FLUX_AUSM 1
+
+#define E3D_FP64 0 /* drop-in: reference FP64 arithmetic */
+#define E3D_FP32 1 /* FP32 bulk, FP64 conserved state and reductions */
+
+typedef struct e3d_case e3d_case;     /* host case: deck + topology + blocks */
+typedef struct e3d_solver e3d_solver; /* device-resident solver over one case */
+
+typedef struct e3d_deck_info {
+	double cfl, gamma, aoa_deg, mach, cmac, criterion, omega, k;
+	int stages, max_iter, smoothing, order;
+	int flux, gradient, limiter; /* E3D_FLUX_*, E3D_GRAD_*, E3D_LIM_* as the reference selects them */
+} e3d_deck_info;
+
+typedef struct e3d_block_info {
+	int n_real, n_all, n_faces, n_nodes, n_markers, n_real_boundaries, n_wall_faces;
+} e3d_block_info;
+
+typedef struct e3d_options {
+	int precision;    /* E3D_FP64 or E3D_FP32 */
+	int carry_w0;     /* -1 default (FP32: on), 0 recompute W0 from primitives, 1 carry FP64 W */
+	int use_graph;    /* 1: one CUDA graph per outer iteration */
+	int device;       /* -1: current device */
+	void* stream;     /* cudaStream_t or NULL (solver creates its own) */
+	int hist_capacity;/* iterations of history buffered on the device (0: 4096) */
+} e3d_options;
+
+/* One outer iteration's post-processing (PostProcessing::process,
+ * PostProcessing/src/PostProcessing.cpp:220-308). */
+typedef struct e3d_iter_record {
+	int iter;
+	double rms[5];  /* rho, u, v, w, p residual norms summed over blocks */
+	double conv[5]; /* log10(rms) - log10(rms at iteration 0) */
+	double cl, cd, cmx, cmy, cmz;
+} e3d_iter_record;
+
+/* ---- errors ---------------------------------------------------------------- */
+const char* e3d_last_error(void);
+const char* e3d_version(void);
+void e3d_default_options(e3d_options* opt);
+
+/* ---- host case ----------------------------------------------------------------
+ * e3d_case_load replaces main.cpp:61-82: Interface::readInputFile
+ * (Solver/src/Interface.cpp:14-237), Interface::readNBlocks (:239-266) and
+ * CompleteMesh::InitializeMyBlocks (DataStructure/src/CompleteMesh.cpp:79-293),
+ * i.e. ConcreteBlockBuilder::preReadMyBlock/readMyBlock/createMyFaces
+ * (BlockBuilder/src/ConcreteBlockBuilder.cpp:22-742), BlockBuilder::setConnectivity
+ * (BlockBuilder/src/BlockBuilder.cpp:147-458) and MetricsInitializer::doInit
+ * (Metrics/src/MetricsInitializer.cpp:27-54).  Relative paths in the deck and
+ * topology are resolved against `workdir` (NULL: the current directory), as
+ * the reference resolves them against its working directory. */
+int e3d_case_load(const char* deck_path, const char* workdir, e3d_case** out);
+int e3d_case_free(e3d_case* c);
+int e3d_case_deck(const e3d_case* c, e3d_deck_info* out);
+int e3d_case_n_blocks(const e3d_case* c, int* n);
+int e3d_case_block_info(const e3d_case* c, int block, e3d_block_info* out);
+/* Copies one per-block array (the reference Block/Cell/Face members) into dst.
+ * count must equal the array length (query with dst == NULL: *count is set).
+ * Float arrays: face_normal, face_area, face_center, r_left, r_right,
+ * cell_volume, cell_center, ls_weights.  Int arrays: face_cells, cell_face_ptr,
+ * cell_faces, cell_cells, wall_faces, marker_kind, marker_size, marker_cells. */
+int e3d_case_get_f64(const e3d_case* c, int block, const char* name, double* dst, int64_t* count);
+int e3d_case_get_i32(const e3d_case* c, int block, const char* name, int32_t* dst, int64_t* count);
+
+/* ---- solver ------------------------------------------------------------------
+ * e3d_solver_create replaces Initializer::initializeSolver
+ * (DataStructure/src/Initializer.cpp:25-50) and the per-block
+ * calculateFreeVariables/initializeFlowField (PrimitiveVariables.cpp:41-69):
+ * uploads the case and sets every cell to freestream.  opt may be NULL. */
+int e3d_solver_create(const e3d_case* c, const e3d_options* opt, e3d_solver** out);
+int e3d_solver_free(e3d_solver* s);
+int e3d_solver_sync(e3d_solver* s);
+int e3d_solver_device_bytes(const e3d_solver* s, int64_t* bytes);
+
+/* Strategy-level calls (FP64 solver only), one per reference method. */
+int e3d_save_w0(e3d_solver* s, int block);           /* Solver::saveW0, Solver/src/Solver.cpp:161-210 */
+int e3d_spectral_radius(e3d_solver* s, int block);   /* Timestep::computeSpectralRadius, Solver/src/Timestep.cpp:26-121 */
+int e3d_timestep(e3d_solver* s, int block);          /* Timestep::computeTimestep, Timestep.cpp:123-148 */
+int e3d_gradients(e3d_solver* s, int block, int kind);/* Gradient::computeGradients: GreenGauss.cpp:12-234, LeastSquares.cpp:12-186 */
+int e3d_limiters(e3d_solver* s, int block, int kind, double omega, double k); /* Limiter::computeLimiters: BarthJespersen.cpp:14-333, Venkatakrishnan.cpp:12-326 */
+int e3d_flux_conv(e3d_solver* s, int block, int scheme);             /* FluxScheme::computeFluxConv, FluxScheme.cpp:16-211; AusmScheme.cpp:647-871 */
+int e3d_flux_diss(e3d_solver* s, int block, int scheme, double beta);/* FluxScheme::computeFluxDiss, RoeScheme.cpp:12-311; AusmScheme.cpp:12-243 */
+int e3d_update_internal(e3d_solver* s, int block, double alpha);    /* Updater::updateInternalBlock, Updater.cpp:12-78 */
+int e3d_update_boundary(e3d_solver* s, int block);                   /* Updater::updateBoundary, Updater.cpp:80-88 */
+int e3d_halo(e3d_solver* s);                                         /* BlockCommunicator::updateBoundaries, MPI/src/BlockCommunicator.cpp:66-270 */
+/* PostProcessing::computeFlowData (PostProcessing.cpp:198-217) for every block:
+ * out[b*10 + 0..4] = sum over real cells of (Rc-Rd)^2 per equation,
+ * out[b*10 + 5..9] = wall sums fy, fx, cmx, cmy, cmz
+ * (Convergence.cpp:27-48, AerodynamicParameters.cpp:163-239). */
+int e3d_flow_data(e3d_solver* s, double* out, int64_t count);
+
+/* Whole outer iterations with fused kernels (Solver::solve body,
+ * Solver/src/Solver.cpp:76-97); records are appended to the history. */
+int e3d_iterate(e3d_solver* s, int n_iter);
+/* Runs until the reference stop test (PostProcessing::checkStopSolver,
+ * PostProcessing.cpp:59-83: iter+1 == max_iter or conv[0] <= criterion),
+ * checking every `check_every` iterations; *iters_done = iterations run. */
+int e3d_solve(e3d_solver* s, int max_iter, double criterion, int check_every, int* iters_done);
+int e3d_history_length(const e3d_solver* s, int* n);
+int e3d_history(const e3d_solver* s, int first, int count, e3d_iter_record* out);
+
+/* State transfer in block-local reference order (FP64 on the host side):
+ * prim/limiter [5][n_all], grad [5][n_all][3], conv_res/diss_res/w0 [5][n_real],
+ * dt/spectral_radius [n_real]. */
+int e3d_state_get(e3d_solver* s, int block, const char* name, double* dst, int64_t count);
+int e3d_state_set(e3d_solver* s, int block, const char* name, const double* src, int64_t count);
+
+/* Measurement: per-kernel CUDA-event times of n eager iterations on the solver
+ * stream.  names: comma-separated kernel names; launches/total_ms/bytes per row. */
+int e3d_time_kernels(e3d_solver* s, int n_iter, char* names, int names_len, int* launches, double* total_ms,
+                     double* bytes_per_launch, int max_rows, int* rows);
+int e3d_launches_per_iteration(const e3d_solver* s, int* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* E3D_H */
