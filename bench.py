@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Throughput of the euler3D residual-and-update path on B200, in cell-iterations/s.
+
+Workload (the second-order configuration): the 80^3 hexahedron bump channel
+split into 6 tetrahedra per hexahedron (3,072,000 tetrahedra), cut into 16
+x-slab topology blocks that all live on one GPU; least-squares gradients,
+Venkatakrishnan limiter (K = 5), Roe flux, Mach 0.7, alpha 1.25 deg, 5-stage
+Runge-Kutta, CFL 1.5; FP32 flux/gradient/limiter arithmetic with the FP64
+conserved state and FP64 norm / force reductions.  The mesh is synthetic
+(seedless deterministic generator, euler3d_b200.meshgen) and goes through the
+reference's file formats (SU2 blocks + .top topology + input deck).
+
+A step is one outer iteration of the solver over every cell of every block
+(5 RK stages, local time step, residual norms, wall forces, inter-block halo).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun): the
+path has no inter-GPU exchange when all blocks of a case live on one GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "cell-iters/s"
+UNIT = "cell-iterations/s"
+WORKLOAD = dict(n=80, blocks=16, order=2, flux="roe", gradient="leastsquares", limiter="venkatakrishnan", k=5.0,
+                omega=2.16e-16, mach=0.7, aoa_deg=1.25, cfl=1.5, stages=5)
+REFDRIVER = os.path.join(HERE, "oracle", "_ref", "e3d_refdriver")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_case(directory: str, n: int, blocks: int) -> str:
+    from euler3d_b200 import meshgen as mg
+
+    w = WORKLOAD
+    deck = mg.Deck(topology="", cfl=w["cfl"], stages=w["stages"], mach=w["mach"], aoa_deg=w["aoa_deg"],
+                   max_iter=1000000, criterion=-15.0, flux=w["flux"], order=w["order"], gradient=w["gradient"],
+                   limiter=w["limiter"], omega=w["omega"], k=w["k"])
+    return mg.write_case(directory, n, blocks, deck=deck)
+
+
+def workload_config(n, blocks, precision):
+    w = WORKLOAD
+    return {"workload": f"bump channel {n}^3 hex x 6 tets ({6 * n ** 3:,} tets), {blocks} slab blocks on one GPU, "
+                        f"{w['gradient']} + {w['limiter']} (K={w['k']:g}) + {w['flux']}, M {w['mach']}, "
+                        f"alpha {w['aoa_deg']}, {w['stages']}-stage RK, CFL {w['cfl']}",
+            "cells": 6 * n ** 3, "blocks": blocks,
+            "arithmetic": "fp32 fluxes/gradients/limiters, fp64 conserved state and reductions"
+            if precision == "fp32" else "fp64 throughout (reference arithmetic)",
+            "l2": "working set (several GB) far larger than the 126 MB L2; no flush needed"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100", "-i", str(gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        self.marks = []
+
+    def mark(self, tag):
+        self.marks.append((tag, time.time()))
+
+    def stop(self):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(", ") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        return rows
+
+    @staticmethod
+    def summarize(rows):
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ CPU baselines
+def run_refdriver(deck: str, blocks: str, iters: int, warmup: int, cwd: str):
+    out = subprocess.run([REFDRIVER, deck, "--iters", str(iters), "--warmup", str(warmup), "--blocks", blocks,
+                          "--quiet"], cwd=cwd, capture_output=True, text=True, check=True, timeout=3600)
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def cpu_baseline_single(deck: str, case_dir: str):
+    """The reference CPU solver on one host core over a bounded sample: block 0
+    of the 16 (192,000 cells) for 2 outer iterations (about 10 s of CPU work)."""
+    if os.path.exists(REFDRIVER):
+        with tempfile.TemporaryDirectory() as wd:
+            _link_case(case_dir, wd)
+            r = run_refdriver(os.path.basename(deck), "0:1", 3, 1, wd)
+        return {"value": r["cell_iters_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"block 0 ({r['cells']:,} cells) of the same workload, {r['iters']} outer iteration(s) "
+                          "after 1 warm-up, reference solver compiled from its sources (serial, -O2), 1 core"}
+    # fallback: the C restatement of the path (pinned bitwise to the reference)
+    sys.path.insert(0, os.path.join(HERE, "tests"))
+    from oracle_c import OracleBlock, OracleCase, params_from_deck
+
+    from euler3d_b200.api import Case
+
+    case = Case(deck)
+    ob = OracleBlock.from_case(case, 0)
+    oc = OracleCase([ob], params_from_deck(case.deck))
+    oc.iterate(1)
+    t = time.perf_counter()
+    oc.iterate(1)
+    dt = time.perf_counter() - t
+    return {"value": ob.n_real / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"block 0 ({ob.n_real:,} cells), 1 outer iteration after 1 warm-up, C restatement, 1 core"}
+
+
+def _link_case(case_dir: str, wd: str):
+    for name in os.listdir(case_dir):
+        if name.endswith((".su2", ".top", ".deck")):
+            os.symlink(os.path.join(case_dir, name), os.path.join(wd, name))
+    os.makedirs(os.path.join(wd, "bin"), exist_ok=True)
+
+
+def run_reference_arm(a, rank: int):
+    """The reference's own CPU solver, all host cores: one process per block
+    range, as the reference distributes blocks over MPI ranks
+    (MPI/src/BlockCommunicator.cpp:20-39); a step is one outer iteration over
+    every block.  Bounded: at most 5 timed steps after at most 1 warm-up."""
+    if rank != 0:
+        return 0
+    n, blocks = a.n, a.blocks
+    if not os.path.exists(REFDRIVER):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/e3d_refdriver was not built (the "
+                                                             "reference sources were absent when build() ran)"}))
+        return 0
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    procs = max(1, min(cores, blocks))
+    steps = max(1, min(a.steps, 5))
+    warm = min(max(a.warmup, 0), 1)
+    with tempfile.TemporaryDirectory() as td:
+        case_dir = os.path.join(td, "case")
+        deck = make_case(case_dir, n, blocks)
+        per = [blocks // procs + (1 if i < blocks % procs else 0) for i in range(procs)]
+        starts = [sum(per[:i]) for i in range(procs)]
+        jobs = []
+        for i in range(procs):
+            wd = os.path.join(td, f"p{i}")
+            os.makedirs(wd)
+            _link_case(case_dir, wd)
+            cmd = [REFDRIVER, os.path.basename(deck), "--iters", str(warm + steps), "--warmup", str(warm),
+                   "--blocks", f"{starts[i]}:{starts[i] + per[i]}", "--quiet"]
+            jobs.append(subprocess.Popen(cmd, cwd=wd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+        res = []
+        for j in jobs:
+            out, _ = j.communicate(timeout=3600)
+            if j.returncode != 0:
+                raise RuntimeError("reference driver failed")
+            res.append(json.loads(out.strip().splitlines()[-1]))
+    cells = sum(r["cells"] for r in res)
+    t = max(r["solve_s"] for r in res)
+    value = cells * steps / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": steps, "warmup": warm,
+            "ms_per_step": 1000.0 * t / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": workload_config(n, blocks, "fp64"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                             "sample": f"{steps} outer iteration(s) of all {blocks} blocks after {warm} warm-up, "
+                                       f"{procs} processes x 1 thread each owning a contiguous block range "
+                                       "(no inter-process halo), reference solver compiled from its sources"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--n", type=int, default=WORKLOAD["n"])
+    ap.add_argument("--blocks", type=int, default=WORKLOAD["blocks"])
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference_arm(a, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    from euler3d_b200 import _lib as L
+    from euler3d_b200.api import Case, Solver
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    warm = max(3, a.warmup)
+    steps = max(1, a.steps)
+    with tempfile.TemporaryDirectory() as td:
+        t0 = time.time()
+        deck = make_case(td, a.n, a.blocks)
+        t1 = time.time()
+        case = Case(deck)
+        t2 = time.time()
+        s = Solver(case, precision=a.precision, device=local, hist_capacity=max(4096, a.steps + 64))
+        t3 = time.time()
+        log(f"[bench] rank {rank}: mesh gen {t1 - t0:.1f}s, case load {t2 - t1:.1f}s, solver setup {t3 - t2:.1f}s, "
+            f"device bytes {s.device_bytes() / 1e9:.2f} GB")
+        cells = sum(case.block_info(b).n_real for b in range(case.n_blocks))
+        clocks = ClockSampler(local)
+        s.iterate(warm)
+        s.sync()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks.mark("start")
+        ms = s.iterate_timed(steps)  # CUDA events on the solver stream around the K graph launches
+        clocks.mark("end")
+        torch.cuda.synchronize()
+        t_ms = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
+        ms = float(t_ms.item())
+        hist = s.history()
+        assert all(abs(x) < 1e300 for x in hist["rms"][:, 0]), "non-finite residual"
+        value = world * cells * steps / (ms / 1000.0)
+        launches = s.launches_per_iteration() * steps
+
+        # per-kernel device times (eager launches with events between kernels)
+        kt = s.time_kernels(min(steps, 10))
+        dom = max(kt, key=lambda k: k["total_ms"])
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        peak = peaks.get("hbm_gbs", 6650.0)
+        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        achieved = dom["bytes_per_launch"] / (dom["total_ms"] / dom["launches"] / 1000.0) / 1e9
+        traffic = None
+        try:
+            tr = json.load(open(os.path.join(HERE, "profiles", "ncu_traffic.json")))
+            traffic = tr.get(f"{a.precision}:{dom['name']}")
+        except Exception:
+            pass
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": traffic, "kernel": dom["name"], "peak_source": peak_src,
+                    "bytes_per_launch": dom["bytes_per_launch"],
+                    "launch_ms": dom["total_ms"] / dom["launches"],
+                    "kernels": {k["name"]: {"launches": k["launches"], "ms": k["total_ms"],
+                                            "gbs": (k["bytes_per_launch"] / (k["total_ms"] / k["launches"] / 1000.0)
+                                                    / 1e9) if k["bytes_per_launch"] else None} for k in kt}}
+
+        # end to end through the C ABI with host buffers: every step imports the
+        # solver state from pinned host memory, runs one outer iteration and
+        # exports the state back (plus the iteration record)
+        nbytes = s.state_bytes()
+        host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        lib = L.lib()
+        L.check(lib.e3d_state_export(s._h, C.c_void_p(host.data_ptr()), nbytes))
+        e2e_steps = max(3, a.e2e_steps)
+        rec = (L.IterRecord * 1)()
+        n_hist = C.c_int()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        te = time.perf_counter()
+        for _ in range(e2e_steps):
+            L.check(lib.e3d_state_import(s._h, C.c_void_p(host.data_ptr()), nbytes))
+            L.check(lib.e3d_iterate(s._h, 1))
+            L.check(lib.e3d_state_export(s._h, C.c_void_p(host.data_ptr()), nbytes))
+            L.check(lib.e3d_history_length(s._h, C.byref(n_hist)))
+            L.check(lib.e3d_history(s._h, n_hist.value - 1, 1, C.cast(rec, C.c_void_p)))
+        te = time.perf_counter() - te
+        t_e = torch.tensor([te], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * cells * e2e_steps / float(t_e.item()), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes + C.sizeof(L.IterRecord), "steps": e2e_steps,
+               "path": "e3d_state_import (pinned host) + e3d_iterate(1) + e3d_state_export + e3d_history, "
+                       "host wall clock"}
+        rows = clocks.stop()
+        # samples whose timestamps fall in the timed region (nvidia-smi prints no
+        # timestamp in this query: keep all samples of the measured run)
+        cl = ClockSampler.summarize(rows)
+
+        cpu = None
+        if rank == 0 and world == 1 and not a.no_cpu_baseline:
+            try:
+                cpu = cpu_baseline_single(deck, td)
+            except Exception as e:  # reported, not fatal: the GPU number stands
+                cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
+            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic",
+            "config": dict(workload_config(a.n, a.blocks, a.precision), parallelism=f"replicas{world}"),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": cl,
+            "final": {"iterations": int(len(hist["iter"])), "ro_conv": float(hist["conv"][-1, 0]),
+                      "cl": float(hist["cl"][-1]), "cd": float(hist["cd"][-1])}}
+    if rank == 0:
+        print(json.dumps(line))
+    s.close()
+    case.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

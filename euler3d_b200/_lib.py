@@ -84,6 +84,10 @@ SIGNATURES = {
     "e3d_flow_data": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "e3d_iterate": ([C.c_void_p, C.c_int], C.c_int),
     "e3d_solve": ([C.c_void_p, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "e3d_iterate_timed": ([C.c_void_p, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "e3d_state_bytes": ([C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
+    "e3d_state_export": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "e3d_state_import": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "e3d_history_length": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "e3d_history": ([C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "e3d_state_get": ([C.c_void_p, C.c_int, C.c_char_p, C.c_void_p, C.c_int64], C.c_int),

@@ -101,6 +101,25 @@ class Solver:
         L.check(L.lib().e3d_solve(self._h, max_iter, criterion, check_every, C.byref(done)))
         return done.value
 
+    def iterate_timed(self, n: int) -> float:
+        """n outer iterations; returns their device time in ms (CUDA events)."""
+        ms = C.c_double()
+        L.check(L.lib().e3d_iterate_timed(self._h, n, C.byref(ms)))
+        return ms.value
+
+    def state_bytes(self) -> int:
+        n = C.c_int64()
+        L.check(L.lib().e3d_state_bytes(self._h, C.byref(n)))
+        return n.value
+
+    def export_state(self, buf) -> None:
+        """Copy the whole solver state into ``buf`` (numpy uint8 array or any
+        object exposing a writable buffer address via ``.ctypes.data``)."""
+        L.check(L.lib().e3d_state_export(self._h, C.c_void_p(buf.ctypes.data), buf.nbytes))
+
+    def import_state(self, buf) -> None:
+        L.check(L.lib().e3d_state_import(self._h, C.c_void_p(buf.ctypes.data), buf.nbytes))
+
     def sync(self) -> None:
         L.check(L.lib().e3d_solver_sync(self._h))
 
@@ -123,6 +142,8 @@ class Solver:
 
     # ---- state
     def _len(self, b: int, name: str) -> int:
+        if not 0 <= b < self.n_blocks:
+            return 0  # the C ABI reports the bad block index
         i = self._info[b]
         if name in _ARRAYS_ALL5:
             return 5 * i.n_all

@@ -263,6 +263,29 @@ int e3d_solve(e3d_solver* s, int max_iter, double criterion, int check_every, in
 	});
 }
 
+int e3d_iterate_timed(e3d_solver* s, int n_iter, double* device_ms) {
+	return guard([&] {
+		const double ms = eng(s).iterate_timed(n_iter);
+		if (device_ms) *device_ms = ms;
+	});
+}
+
+int e3d_state_bytes(const e3d_solver* s, int64_t* bytes) {
+	if (!s || !s->eng || !bytes) return fail(E3D_ERR_ARG, "null argument");
+	*bytes = (int64_t)s->eng->state_bytes();
+	return E3D_OK;
+}
+
+int e3d_state_export(e3d_solver* s, void* host, int64_t bytes) {
+	if (bytes < 0) return fail(E3D_ERR_ARG, "negative size");
+	return guard([&] { eng(s).export_state(host, (size_t)bytes); });
+}
+
+int e3d_state_import(e3d_solver* s, const void* host, int64_t bytes) {
+	if (bytes < 0) return fail(E3D_ERR_ARG, "negative size");
+	return guard([&] { eng(s).import_state(host, (size_t)bytes); });
+}
+
 int e3d_history_length(const e3d_solver* s, int* n) {
 	if (!s || !s->eng || !n) return fail(E3D_ERR_ARG, "null argument");
 	*n = (int)s->eng->history().size();

@@ -609,6 +609,109 @@ void Engine::iterate(int n) {
 	else run_iterations(f32_, n);
 }
 
+double Engine::iterate_timed(int n) {
+	if (n < 0) throw Error(E3D_ERR_ARG, "negative iteration count");
+	if (!started_) halo();
+	if ((int)opt_.hist_capacity - dev_iter_ < n) collect_history(total_iter_, dev_iter_);
+	if ((int)opt_.hist_capacity < n) throw Error(E3D_ERR_LIMIT, "timed run longer than the history capacity");
+	cudaEvent_t e0, e1;
+	cuda_ok(cudaEventCreate(&e0), "event");
+	cuda_ok(cudaEventCreate(&e1), "event");
+	cuda_ok(cudaEventRecord(e0, st_), "event");
+	const int stages = (int)alpha_.size();
+	for (int i = 0; i < n; i++) {
+		if (opt_.use_graph) {
+			if (!graph_[cur_]) {
+				cudaGraph_t g;
+				cuda_ok(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal), "capture");
+				if (opt_.precision == PREC_FP64) iteration_body<double>(f64_, cur_, nullptr);
+				else iteration_body<float>(f32_, cur_, nullptr);
+				cuda_ok(cudaStreamEndCapture(st_, &g), "capture");
+				cuda_ok(cudaGraphInstantiate(&graph_[cur_], g, 0), "graph instantiate");
+				cudaGraphDestroy(g);
+			}
+			cuda_ok(cudaGraphLaunch(graph_[cur_], st_), "graph launch");
+		} else {
+			if (opt_.precision == PREC_FP64) iteration_body<double>(f64_, cur_, nullptr);
+			else iteration_body<float>(f32_, cur_, nullptr);
+			check("iteration");
+		}
+		cur_ ^= (stages & 1);
+	}
+	cuda_ok(cudaEventRecord(e1, st_), "event");
+	cuda_ok(cudaEventSynchronize(e1), "event sync");
+	float ms = 0.f;
+	cuda_ok(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	dev_iter_ += n;
+	collect_history(total_iter_, dev_iter_);
+	return (double)ms;
+}
+
+namespace {
+struct StateHeader {
+	char magic[8];
+	int32_t precision, n_blocks;
+	int64_t NA, NR, iters;
+	int32_t have_rms0, carry;
+	double rms0[5];
+};
+}  // namespace
+
+size_t Engine::state_bytes() const {
+	const size_t b = opt_.precision == PREC_FP64 ? 8 : 4;
+	return sizeof(StateHeader) + 5 * (size_t)NA_ * b + 5 * (size_t)NR_ * 8;
+}
+
+// Layout: header, then primitives [5][NA] in device order (real cells of every
+// block, then ghost cells of every block) and precision, then FP64 W0 [5][NR].
+void Engine::export_state(void* host, size_t bytes) {
+	if (!host || bytes < state_bytes()) throw Error(E3D_ERR_ARG, "state buffer too small");
+	StateHeader h{};
+	std::memcpy(h.magic, "E3DSTAT1", 8);
+	h.precision = opt_.precision;
+	h.n_blocks = nb_;
+	h.NA = NA_;
+	h.NR = NR_;
+	h.iters = total_iter_ + dev_iter_;
+	h.have_rms0 = have_rms0_ ? 1 : 0;
+	h.carry = carry_;
+	for (int q = 0; q < 5; q++) h.rms0[q] = rms0_[q];
+	std::memcpy(host, &h, sizeof(h));
+	char* p = static_cast<char*>(host) + sizeof(h);
+	const size_t pb = (opt_.precision == PREC_FP64 ? 8 : 4) * 5 * (size_t)NA_;
+	const void* P = opt_.precision == PREC_FP64 ? (const void*)(cur_ ? f64_.P1.p : f64_.P0.p)
+	                                            : (const void*)(cur_ ? f32_.P1.p : f32_.P0.p);
+	cuda_ok(cudaMemcpyAsync(p, P, pb, cudaMemcpyDeviceToHost, st_), "export");
+	cuda_ok(cudaMemcpyAsync(p + pb, W0_.p, 5 * (size_t)NR_ * 8, cudaMemcpyDeviceToHost, st_), "export");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+}
+
+void Engine::import_state(const void* host, size_t bytes) {
+	if (!host || bytes < sizeof(StateHeader)) throw Error(E3D_ERR_ARG, "state buffer too small");
+	StateHeader h;
+	std::memcpy(&h, host, sizeof(h));
+	if (std::memcmp(h.magic, "E3DSTAT1", 8) != 0) throw Error(E3D_ERR_FORMAT, "not an e3d state buffer");
+	if (h.precision != opt_.precision || h.NA != NA_ || h.NR != NR_ || h.n_blocks != nb_)
+		throw Error(E3D_ERR_ARG, "state buffer is for another case or precision");
+	if (bytes < state_bytes()) throw Error(E3D_ERR_ARG, "state buffer truncated");
+	const char* p = static_cast<const char*>(host) + sizeof(h);
+	const size_t pb = (opt_.precision == PREC_FP64 ? 8 : 4) * 5 * (size_t)NA_;
+	void* P = opt_.precision == PREC_FP64 ? (void*)(cur_ ? f64_.P1.p : f64_.P0.p) : (void*)(cur_ ? f32_.P1.p : f32_.P0.p);
+	void* Q = opt_.precision == PREC_FP64 ? (void*)(cur_ ? f64_.P0.p : f64_.P1.p) : (void*)(cur_ ? f32_.P0.p : f32_.P1.p);
+	cuda_ok(cudaMemcpyAsync(P, p, pb, cudaMemcpyHostToDevice, st_), "import");
+	// the other buffer too: ghost cells that no stage rewrites must agree in both
+	cuda_ok(cudaMemcpyAsync(Q, P, pb, cudaMemcpyDeviceToDevice, st_), "import");
+	cuda_ok(cudaMemcpyAsync(W0_.p, p + pb, 5 * (size_t)NR_ * 8, cudaMemcpyHostToDevice, st_), "import");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	if (dev_iter_) collect_history(total_iter_, dev_iter_);
+	total_iter_ = (int)h.iters;
+	have_rms0_ = h.have_rms0 != 0;
+	for (int q = 0; q < 5; q++) rms0_[q] = h.rms0[q];
+	started_ = true;
+}
+
 // Pulls the device history records, converts them to the reference's mesh-level
 // quantities, and resets the device counter.
 void Engine::collect_history(int first_iter, int n) {

@@ -63,6 +63,14 @@ public:
 
 	// --- whole outer iterations (fused kernels); appends to history()
 	void iterate(int n_iter);
+	// iterate with CUDA events recorded on the engine stream around the launches;
+	// returns the device time of the n iterations in milliseconds
+	double iterate_timed(int n_iter);
+	// checkpoint: the complete solver state (current primitives in device
+	// precision, FP64 W0, iteration count, iteration-0 norms) to / from a host buffer
+	size_t state_bytes() const;
+	void export_state(void* host, size_t bytes);
+	void import_state(const void* host, size_t bytes);
 	// run until the reference stop test (max_iter or criterion) fires
 	int solve(int max_iter, double criterion, int check_every);
 

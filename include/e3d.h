@@ -137,6 +137,9 @@ int e3d_iterate(e3d_solver* s, int n_iter);
  * PostProcessing.cpp:59-83: iter+1 == max_iter or conv[0] <= criterion),
  * checking every `check_every` iterations; *iters_done = iterations run. */
 int e3d_solve(e3d_solver* s, int max_iter, double criterion, int check_every, int* iters_done);
+/* e3d_iterate with CUDA events around the launches on the solver stream:
+ * *device_ms = device time of the n iterations. */
+int e3d_iterate_timed(e3d_solver* s, int n_iter, double* device_ms);
 int e3d_history_length(const e3d_solver* s, int* n);
 int e3d_history(const e3d_solver* s, int first, int count, e3d_iter_record* out);
 
@@ -145,6 +148,16 @@ int e3d_history(const e3d_solver* s, int first, int count, e3d_iter_record* out)
  * dt/spectral_radius [n_real]. */
 int e3d_state_get(e3d_solver* s, int block, const char* name, double* dst, int64_t count);
 int e3d_state_set(e3d_solver* s, int block, const char* name, const double* src, int64_t count);
+
+/* Checkpoint / restart of the whole solver state (the reference's restart
+ * writer is an empty stub, PostProcessing/src/OutputTecplot.cpp:475-494):
+ * current primitives of every cell in the solver precision, the FP64
+ * conservative state W0, the iteration count and the iteration-0 norms.
+ * Query the size with e3d_state_bytes; export copies device -> host buffer
+ * (pinned memory makes the copy faster), import the reverse. */
+int e3d_state_bytes(const e3d_solver* s, int64_t* bytes);
+int e3d_state_export(e3d_solver* s, void* host, int64_t bytes);
+int e3d_state_import(e3d_solver* s, const void* host, int64_t bytes);
 
 /* Measurement: per-kernel CUDA-event times of n eager iterations on the solver
  * stream.  names: comma-separated kernel names; launches/total_ms/bytes per row. */

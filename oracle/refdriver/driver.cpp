@@ -8,8 +8,10 @@
 // the same calls in the same order and copies arrays out.
 //
 //   e3d_refdriver DECK [--iters N] [--dump-dir DIR] [--dump-init] [--dump-stages]
-//                      [--dump-every K] [--history FILE] [--blocks A:B] [--quiet]
+//                      [--dump-every K] [--history FILE] [--blocks A:B] [--warmup W] [--quiet]
 //
+// --warmup W runs W outer iterations before the timer starts (the reported
+// iterations and rate cover the remaining --iters minus W).
 // --blocks A:B owns only blocks [A,B) (the reference's per-rank block range,
 // BlockCommunicator.cpp:284-294); connexions touching other blocks are then not
 // exchanged.  That mode exists to time bounded samples on several host cores.
@@ -51,6 +53,7 @@ struct Options {
 	bool dump_init = false;
 	bool dump_stages = false;
 	int dump_every = 0;
+	int warmup = 0;
 	std::string history;
 	int block_lo = -1, block_hi = -1;
 	bool quiet = false;
@@ -217,7 +220,7 @@ int main(int argc, char** argv) {
 	Options o;
 	if (argc < 2) {
 		std::cerr << "usage: e3d_refdriver DECK [--iters N] [--dump-dir DIR] [--dump-init] [--dump-stages] "
-		             "[--dump-every K] [--history FILE] [--blocks A:B] [--quiet]" << std::endl;
+		             "[--dump-every K] [--history FILE] [--blocks A:B] [--warmup W] [--quiet]" << std::endl;
 		return 2;
 	}
 	o.deck = argv[1];
@@ -232,6 +235,7 @@ int main(int argc, char** argv) {
 		else if (a == "--dump-init") o.dump_init = true;
 		else if (a == "--dump-stages") o.dump_stages = true;
 		else if (a == "--dump-every") o.dump_every = std::atoi(next().c_str());
+		else if (a == "--warmup") o.warmup = std::atoi(next().c_str());
 		else if (a == "--history") o.history = next();
 		else if (a == "--blocks") {
 			std::string v = next();
@@ -292,6 +296,7 @@ int main(int argc, char** argv) {
 	RungeKutta* rk = solver->runge_kutta_;
 	auto t0 = std::chrono::high_resolution_clock::now();
 	for (int it = 0; it < iters; it++) {
+		if (it == o.warmup) t0 = std::chrono::high_resolution_clock::now();
 		for (int i = 0; i < mesh->n_blocks_in_process_; i++) {  // Solver.cpp:83-91
 			Block* b = mesh->all_blocks_[mesh->my_blocks_[i]];
 			solver->saveW0(b);
@@ -328,8 +333,9 @@ int main(int argc, char** argv) {
 	long long cells = 0;
 	for (int i = 0; i < mesh->n_blocks_in_process_; i++) cells += mesh->all_blocks_[mesh->my_blocks_[i]]->n_real_cells_in_block_;
 	const double solve_s = std::chrono::duration<double>(t1 - t0).count();
+	const int timed = iters > o.warmup ? iters - o.warmup : 0;
 	std::printf("{\"cells\": %lld, \"iters\": %d, \"solve_s\": %.6f, \"preprocess_s\": %.6f, \"cell_iters_per_s\": %.6g}\n",
-	            cells, iters, solve_s, std::chrono::duration<double>(t_pre1 - t_pre0).count(),
-	            solve_s > 0 ? (double)cells * iters / solve_s : 0.0);
+	            cells, timed, solve_s, std::chrono::duration<double>(t_pre1 - t_pre0).count(),
+	            solve_s > 0 ? (double)cells * timed / solve_s : 0.0);
 	return 0;
 }
