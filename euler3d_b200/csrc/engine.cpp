@@ -275,6 +275,7 @@ void Engine::build(const HostCase& hc) {
 	partial_.alloc((size_t)nb_ * max_chunks_ * 5);
 	hist_d_.alloc(opt_.hist_capacity * (size_t)nb_ * 10);
 	fd_hist_.alloc((size_t)nb_ * 10);
+	wall_terms_.alloc(5 * std::max<size_t>(1, wall_face_.n));
 	iter_d_.alloc(1);
 	bad_d_.alloc(1);
 	zero_d_.alloc(1);
@@ -287,8 +288,10 @@ void Engine::init_state() {
 	// all cells, ghosts included, start at freestream
 	// (PrimitiveVariables::initializeFlowField, PrimitiveVariables.cpp:58-69);
 	// residuals, W0, gradients and limiters start at zero (value-initialised arrays)
-	std::vector<double> P(5 * (size_t)NA_);
-	for (int q = 0; q < 5; q++) std::fill(P.begin() + (size_t)q * NA_, P.begin() + (size_t)(q + 1) * NA_, ph_.free[q]);
+	std::vector<double> P(5 * (size_t)NA_);  // packed: [NA] x (rho,u,v,w), then [NA] p
+	for (int c = 0; c < NA_; c++)
+		for (int q = 0; q < 4; q++) P[4 * (size_t)c + q] = ph_.free[q];
+	std::fill(P.begin() + 4 * (size_t)NA_, P.end(), ph_.free[4]);
 	std::vector<double> zR(5 * (size_t)NR_, 0.0);
 	if (opt_.precision == PREC_FP64) {
 		f64_.P0.upload(P);
@@ -482,8 +485,9 @@ void Engine::halo() {
 }
 
 static ReduceArgs make_reduce(int NR, int NA, int nb, const int* roff, int chunk, int max_chunks, double* partial,
-                              const int* woff, const int* wface, const int* flr, const double* S, const double* fc,
-                              double denom, double* hist, const int* d_iter, int* d_bad) {
+                              const int* woff, const int* wface, int n_wall, double* wall_terms, const int* flr,
+                              const double* S, const double* fc, double denom, double* hist, const int* d_iter,
+                              int* d_bad) {
 	ReduceArgs a{};
 	a.NR = NR;
 	a.NA = NA;
@@ -494,6 +498,8 @@ static ReduceArgs make_reduce(int NR, int NA, int nb, const int* roff, int chunk
 	a.partial = partial;
 	a.wall_off = woff;
 	a.wall_face = wface;
+	a.n_wall = n_wall;
+	a.wall_terms = wall_terms;
 	a.face_lr = flr;
 	a.S = S;
 	a.fc = fc;
@@ -507,7 +513,8 @@ static ReduceArgs make_reduce(int NR, int NA, int nb, const int* roff, int chunk
 
 void Engine::flow_data(std::vector<double>& out) {
 	ReduceArgs a = make_reduce(NR_, NA_, nb_, roff_d_.p, chunk_, max_chunks_, partial_.p, wall_off_.p, wall_face_.p,
-	                           face_lr_.p, S_.p, fc_.p, denom_, fd_hist_.p, zero_d_.p, bad_d_.p);
+	                           (int)wall_face_.n, wall_terms_.p, face_lr_.p, S_.p, fc_.p, denom_, fd_hist_.p, zero_d_.p,
+	                           bad_d_.p);
 	if (opt_.precision == PREC_FP64)
 		launch_reduce<double>(a, f64_.Rc.p, f64_.Rd.p, cur_ ? f64_.P1.p : f64_.P0.p, st_);
 	else
@@ -561,7 +568,8 @@ void Engine::iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* m
 		p ^= 1;
 	}
 	ReduceArgs a = make_reduce(NR_, NA_, nb_, roff_d_.p, chunk_, max_chunks_, partial_.p, wall_off_.p, wall_face_.p,
-	                           face_lr_.p, S_.p, fc_.p, denom_, hist_d_.p, iter_d_.p, bad_d_.p);
+	                           (int)wall_face_.n, wall_terms_.p, face_lr_.p, S_.p, fc_.p, denom_, hist_d_.p, iter_d_.p,
+	                           bad_d_.p);
 	launch_reduce<T>(a, f.Rc.p, f.Rd.p, p ? f.P1.p : f.P0.p, st_);
 	launch_halo<T>((int)halo_dst_.n, halo_dst_.p, halo_src_.p, NA_, p ? f.P1.p : f.P0.p, p ? f.P0.p : f.P1.p, st_);
 	launch_iter_advance(iter_d_.p, st_);
@@ -787,6 +795,37 @@ void d2h_rows(const T* dev, int ld, int rows, int begin, int count, std::vector<
 		for (int i = 0; i < count; i++) out[out_off + (size_t)q * out_ld + i] = (double)tmp[i];
 	}
 }
+// Packed five-variable arrays (kernels.cuh ld5/st5): [n] x (rho,u,v,w) then [n] p.
+template <class T>
+void d2h_packed(const T* dev, int n, int begin, int count, std::vector<double>& out, size_t out_off, int out_ld,
+                cudaStream_t st) {
+	if (count == 0) return;
+	std::vector<T> v4(4 * (size_t)count), p((size_t)count);
+	cuda_ok(cudaMemcpyAsync(v4.data(), dev + 4 * (size_t)begin, 4 * (size_t)count * sizeof(T), cudaMemcpyDeviceToHost,
+	                        st),
+	        "d2h");
+	cuda_ok(cudaMemcpyAsync(p.data(), dev + 4 * (size_t)n + begin, count * sizeof(T), cudaMemcpyDeviceToHost, st), "d2h");
+	cuda_ok(cudaStreamSynchronize(st), "sync");
+	for (int i = 0; i < count; i++) {
+		for (int q = 0; q < 4; q++) out[out_off + (size_t)q * out_ld + i] = (double)v4[4 * (size_t)i + q];
+		out[out_off + 4 * (size_t)out_ld + i] = (double)p[i];
+	}
+}
+template <class T>
+void h2d_packed(T* dev, int n, int begin, int count, const std::vector<double>& in, size_t in_off, int in_ld,
+                cudaStream_t st) {
+	if (count == 0) return;
+	std::vector<T> v4(4 * (size_t)count), p((size_t)count);
+	for (int i = 0; i < count; i++) {
+		for (int q = 0; q < 4; q++) v4[4 * (size_t)i + q] = (T)in[in_off + (size_t)q * in_ld + i];
+		p[i] = (T)in[in_off + 4 * (size_t)in_ld + i];
+	}
+	cuda_ok(cudaMemcpyAsync(dev + 4 * (size_t)begin, v4.data(), 4 * (size_t)count * sizeof(T), cudaMemcpyHostToDevice,
+	                        st),
+	        "h2d");
+	cuda_ok(cudaMemcpyAsync(dev + 4 * (size_t)n + begin, p.data(), count * sizeof(T), cudaMemcpyHostToDevice, st), "h2d");
+	cuda_ok(cudaStreamSynchronize(st), "sync");
+}
 template <class T>
 void h2d_rows(T* dev, int ld, int rows, int begin, int count, const std::vector<double>& in, size_t in_off, int in_ld,
               cudaStream_t st) {
@@ -818,9 +857,14 @@ void Engine::get(const std::string& name, int b, std::vector<double>& out) {
 		out.assign((size_t)rows * nr, 0.0);
 		d2h_rows(dev, NR_, rows, r0, nr, out, 0, nr, st_);
 	};
+	auto packed_all = [&](auto* dev) {
+		out.assign((size_t)5 * na, 0.0);
+		d2h_packed(dev, NA_, r0, nr, out, 0, na, st_);
+		d2h_packed(dev, NA_, g0, ng, out, nr, na, st_);
+	};
 	if (name == "prim") {
-		if (f64) rows_all(5, cur_ ? f64_.P1.p : f64_.P0.p);
-		else rows_all(5, cur_ ? f32_.P1.p : f32_.P0.p);
+		if (f64) packed_all(cur_ ? f64_.P1.p : f64_.P0.p);
+		else packed_all(cur_ ? f32_.P1.p : f32_.P0.p);
 	} else if (name == "conv_res") {
 		if (f64) rows_real(5, f64_.Rc.p);
 		else rows_real(5, f32_.Rc.p);
@@ -867,14 +911,19 @@ void Engine::set(const std::string& name, int b, const std::vector<double>& in) 
 		if (in.size() != (size_t)rows * nr) throw Error(E3D_ERR_ARG, name + ": wrong length");
 		h2d_rows(dev, NR_, rows, r0, nr, in, 0, nr, st_);
 	};
+	auto put_packed = [&](auto* dev) {
+		if (in.size() != (size_t)5 * na) throw Error(E3D_ERR_ARG, name + ": wrong length");
+		h2d_packed(dev, NA_, r0, nr, in, 0, na, st_);
+		h2d_packed(dev, NA_, g0, ng, in, nr, na, st_);
+	};
 	if (name == "prim") {
 		// both ping-pong buffers, so ghost cells that no stage rewrites stay consistent
 		if (f64) {
-			put_all(5, f64_.P0.p);
-			put_all(5, f64_.P1.p);
+			put_packed(f64_.P0.p);
+			put_packed(f64_.P1.p);
 		} else {
-			put_all(5, f32_.P0.p);
-			put_all(5, f32_.P1.p);
+			put_packed(f32_.P0.p);
+			put_packed(f32_.P1.p);
 		}
 	} else if (name == "conv_res") {
 		if (f64) put_real(5, f64_.Rc.p);

@@ -146,7 +146,7 @@ private:
 	Fused<float> f32_;
 	int cur_ = 0;  // which of P0/P1 holds the current state
 	// reductions
-	DevBuf<double> partial_, hist_d_, fd_hist_;
+	DevBuf<double> partial_, hist_d_, fd_hist_, wall_terms_;
 	DevBuf<int> iter_d_, bad_d_, zero_d_;
 	bool started_ = false;
 	int chunk_ = 0, max_chunks_ = 0;

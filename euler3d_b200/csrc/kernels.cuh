@@ -16,23 +16,40 @@ namespace e3d {
 // Internal linkage: k64.cu and k32.cu each compile their own copy.
 namespace {
 
+// Five-variable arrays use a packed layout: [n] vectors of (rho, u, v, w)
+// followed by [n] p.  A gather of one cell's state touches two memory sectors
+// (one 16/32-byte vector + one scalar) instead of five.
+template <class T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+	using type = float4;
+};
+template <>
+struct Vec4<double> {
+	using type = double4;
+};
+
 template <class T>
 __device__ __forceinline__ Q5<T> ld5(const T* __restrict__ P, int n, int c) {
+	const typename Vec4<T>::type a = reinterpret_cast<const typename Vec4<T>::type*>(P)[c];
 	Q5<T> q;
-	q.r = P[c];
-	q.u = P[n + c];
-	q.v = P[2 * n + c];
-	q.w = P[3 * n + c];
-	q.p = P[4 * n + c];
+	q.r = a.x;
+	q.u = a.y;
+	q.v = a.z;
+	q.w = a.w;
+	q.p = P[4 * (size_t)n + c];
 	return q;
 }
 template <class T>
 __device__ __forceinline__ void st5(T* __restrict__ P, int n, int c, const Q5<T>& q) {
-	P[c] = q.r;
-	P[n + c] = q.u;
-	P[2 * n + c] = q.v;
-	P[3 * n + c] = q.w;
-	P[4 * n + c] = q.p;
+	typename Vec4<T>::type a;
+	a.x = q.r;
+	a.y = q.u;
+	a.z = q.v;
+	a.w = q.w;
+	reinterpret_cast<typename Vec4<T>::type*>(P)[c] = a;
+	P[4 * (size_t)n + c] = q.p;
 }
 template <class T>
 __device__ __forceinline__ T& qv(Q5<T>& q, int v) { return (&q.r)[v]; }
@@ -309,47 +326,119 @@ __global__ void k_halo(int n, const int* __restrict__ dst, const int* __restrict
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n) return;
 	const int d = dst[t], o = src[t];
-	for (int v = 0; v < 5; v++) {
-		const T x = b0[v * NA + o];
-		b0[v * NA + d] = x;
-		if (b1) b1[v * NA + d] = x;
-	}
+	const Q5<T> q = ld5(b0, NA, o);
+	st5(b0, NA, d, q);
+	if (b1) st5(b1, NA, d, q);
 }
 
 // ===================================================================== fused
+// Slot data of one real cell.  NSL = 4 is the all-tetrahedron fast path:
+// slots of cell c are 4c..4c+3, so per-slot arrays load as vectors.  NSL = 0
+// reads the slot range from slot_ptr (any cell type).
+template <class T, int NSL>
+struct SlotRange {
+	int s0, n;
+	__device__ __forceinline__ SlotRange(const FusedView<T>& v, int c) {
+		if (NSL == 4) {
+			s0 = 4 * c;
+			n = 4;
+		} else {
+			s0 = v.slot_ptr[c];
+			n = v.slot_ptr[c + 1] - s0;
+		}
+	}
+};
+constexpr int MAXSL = 6;  // hexahedra
+
+// 3 consecutive values per slot (r-vectors, LS weights, signed area vectors)
+template <class T, int NSL>
+__device__ __forceinline__ void load3(const T* __restrict__ a, const SlotRange<T, NSL>& r, T o[MAXSL][3]) {
+	if (NSL == 4 && sizeof(T) == 4) {
+		const float4* p = reinterpret_cast<const float4*>(a + 3 * (size_t)r.s0);
+		const float4 x = __ldg(p), y = __ldg(p + 1), z = __ldg(p + 2);
+		const float f[12] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w, z.x, z.y, z.z, z.w};
+#pragma unroll
+		for (int k = 0; k < 4; k++)
+			for (int d = 0; d < 3; d++) o[k][d] = (T)f[3 * k + d];
+	} else if (NSL == 4) {
+		const double2* p = reinterpret_cast<const double2*>(a + 3 * (size_t)r.s0);
+		double f[12];
+#pragma unroll
+		for (int i = 0; i < 6; i++) {
+			const double2 t = __ldg(p + i);
+			f[2 * i] = t.x;
+			f[2 * i + 1] = t.y;
+		}
+#pragma unroll
+		for (int k = 0; k < 4; k++)
+			for (int d = 0; d < 3; d++) o[k][d] = (T)f[3 * k + d];
+	} else {
+		for (int k = 0; k < r.n; k++)
+			for (int d = 0; d < 3; d++) o[k][d] = a[3 * (size_t)(r.s0 + k) + d];
+	}
+}
+template <class T, int NSL>
+__device__ __forceinline__ void load_int(const int* __restrict__ a, const SlotRange<T, NSL>& r, int o[MAXSL]) {
+	if (NSL == 4) {
+		const int4 x = __ldg(reinterpret_cast<const int4*>(a + r.s0));
+		o[0] = x.x;
+		o[1] = x.y;
+		o[2] = x.z;
+		o[3] = x.w;
+	} else {
+		for (int k = 0; k < r.n; k++) o[k] = a[r.s0 + k];
+	}
+}
+// face normal + area of each slot (face orientation)
+template <class T, int NSL>
+__device__ __forceinline__ void load_geo(const T* __restrict__ a, const SlotRange<T, NSL>& r, T o[MAXSL][4]) {
+	const typename Vec4<T>::type* p = reinterpret_cast<const typename Vec4<T>::type*>(a) + r.s0;
+#pragma unroll
+	for (int k = 0; k < (NSL == 4 ? 4 : MAXSL); k++) {
+		if (NSL != 4 && k >= r.n) break;
+		const typename Vec4<T>::type t = p[k];
+		o[k][0] = t.x;
+		o[k][1] = t.y;
+		o[k][2] = t.z;
+		o[k][3] = t.w;
+	}
+}
+
+#define E3D_SLOTS(k, r) for (int k = 0; k < (NSL == 4 ? 4 : MAXSL); k++) if (NSL == 4 || k < r.n)
+
 // Pass 1 of a stage, one thread per real cell: gradient, limiter and MUSCL
 // face states of the cell and of its ghost cells.  FIRST additionally computes
 // W0 (unless carried) and the local time step from the stage-0 state.
-template <class T, int GRAD, int LIM, bool FIRST>
-__global__ void __launch_bounds__(128) k_recon(FusedView<T> v, Physics ph, int carry_w0) {
+template <class T, int GRAD, int LIM, bool FIRST, int NSL>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_recon(FusedView<T> v, Physics ph, int carry_w0) {
 	const int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= v.NR) return;
-	const int s0 = v.tet4 ? 4 * c : v.slot_ptr[c];
-	const int s1 = v.tet4 ? s0 + 4 : v.slot_ptr[c + 1];
+	const SlotRange<T, NSL> sr(v, c);
 	const Q5<T> q0 = ld5(v.Pin, v.NA, c);
+	int nb[MAXSL];
+	load_int<T, NSL>(v.slot_nbr, sr, nb);
+	T w[MAXSL][3];
+	if (GRAD == GRAD_GREEN_GAUSS) load3<T, NSL>(v.sS, sr, w);
+	else load3<T, NSL>(v.lsw, sr, w);
 	T gr[5][3];
 	for (int q = 0; q < 5; q++) gr[q][0] = gr[q][1] = gr[q][2] = T(0.0);
 	Q5<T> mx = q0, mn = q0;
-	for (int k = s0; k < s1; k++) {
-		const Q5<T> qn = ld5(v.Pin, v.NA, v.slot_nbr[k]);
-		if (GRAD == GRAD_GREEN_GAUSS) {
-			const T n0 = v.sS[3 * k], n1 = v.sS[3 * k + 1], n2 = v.sS[3 * k + 2];
-			for (int q = 0; q < 5; q++) {
-				const T a = T(0.5) * (qv(q0, q) + qv(qn, q));
-				gr[q][0] += a * n0;
-				gr[q][1] += a * n1;
-				gr[q][2] += a * n2;
-			}
-		} else {
-			const T w0 = v.lsw[3 * k], w1 = v.lsw[3 * k + 1], w2 = v.lsw[3 * k + 2];
-			for (int q = 0; q < 5; q++) {
-				const T dq = qv(qn, q) - qv(q0, q);
-				gr[q][0] += w0 * dq;
-				gr[q][1] += w1 * dq;
-				gr[q][2] += w2 * dq;
-			}
-		}
+#pragma unroll
+	E3D_SLOTS(k, sr) {
+		const Q5<T> qn = ld5(v.Pin, v.NA, nb[k]);
 		for (int q = 0; q < 5; q++) {
+			if (GRAD == GRAD_GREEN_GAUSS) {
+				// 0.5*(q_L+q_R)*(+-S): addition commutes, so owner/neighbour order is exact
+				const T a = T(0.5) * (qv(q0, q) + qv(qn, q));
+				gr[q][0] += a * w[k][0];
+				gr[q][1] += a * w[k][1];
+				gr[q][2] += a * w[k][2];
+			} else {
+				const T dq = qv(qn, q) - qv(q0, q);
+				gr[q][0] += w[k][0] * dq;
+				gr[q][1] += w[k][1] * dq;
+				gr[q][2] += w[k][2] * dq;
+			}
 			if (qv(qn, q) > qv(mx, q)) qv(mx, q) = qv(qn, q);
 			if (qv(qn, q) < qv(mn, q)) qv(mn, q) = qv(qn, q);
 		}
@@ -358,55 +447,64 @@ __global__ void __launch_bounds__(128) k_recon(FusedView<T> v, Physics ph, int c
 	if (GRAD == GRAD_GREEN_GAUSS)
 		for (int d = 0; d < 3; d++)
 			for (int q = 0; q < 5; q++) gr[q][d] /= V;
-	T phi[5], dmax[5], dmin[5];
-	for (int q = 0; q < 5; q++) {
-		dmax[q] = qv(mx, q) - qv(q0, q);
-		dmin[q] = qv(mn, q) - qv(q0, q);
-		phi[q] = T(INFINITY);
-	}
+	T rv[MAXSL][3];
+	load3<T, NSL>(v.srv, sr, rv);
+	T phi[5];
 	const T eps2 = T(ph.k3) * V;
-	for (int k = s0; k < s1; k++) {
-		const T r0 = v.srv[3 * k], r1 = v.srv[3 * k + 1], r2 = v.srv[3 * k + 2];
-		for (int q = 0; q < 5; q++) {
+	for (int q = 0; q < 5; q++) {
+		const T dmax = qv(mx, q) - qv(q0, q), dmin = qv(mn, q) - qv(q0, q);
+		phi[q] = T(INFINITY);
+#pragma unroll
+		E3D_SLOTS(k, sr) {
 			T d2 = T(0.0);
-			d2 += gr[q][0] * r0;
-			d2 += gr[q][1] * r1;
-			d2 += gr[q][2] * r2;
-			const T lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2, dmax[q], dmin[q], T(ph.omega))
-			                                          : limiter_venkat_face(d2, dmax[q], dmin[q], eps2);
+			d2 += gr[q][0] * rv[k][0];
+			d2 += gr[q][1] * rv[k][1];
+			d2 += gr[q][2] * rv[k][2];
+			const T lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2, dmax, dmin, T(ph.omega))
+			                                          : limiter_venkat_face(d2, dmax, dmin, eps2);
 			if (lf < phi[q]) phi[q] = lf;
 		}
 	}
-	for (int k = s0; k < s1; k++) {
-		const T r0 = v.srv[3 * k], r1 = v.srv[3 * k + 1], r2 = v.srv[3 * k + 2];
-		for (int q = 0; q < 5; q++) v.FS[q * v.NS + k] = recon(qv(q0, q), phi[q], gr[q][0], gr[q][1], gr[q][2], r0, r1, r2);
-		const int nb = v.slot_nbr[k];
-		if (nb < v.NR) continue;
-		// ghost cell of this face: its gradient, limiter (its only neighbour is c)
-		// and face state
-		int ms = v.slot_mate[k];
-		ms = ms >= 0 ? ms : ~ms;
-		const Q5<T> qg = ld5(v.Pin, v.NA, nb);
-		const T nx = v.sgeo[4 * k], ny = v.sgeo[4 * k + 1], nz = v.sgeo[4 * k + 2];
-		const T g0 = v.srv[3 * ms], g1 = v.srv[3 * ms + 1], g2 = v.srv[3 * ms + 2];
-		const bool refl = v.grefl[nb - v.NR] != 0;
-		const T eps2g = T(ph.k3) * v.vol[nb];
-		for (int q = 0; q < 5; q++) {
-			T gg[3] = {T(0.0), T(0.0), T(0.0)};
-			if (refl) reflect_grad(gr[q], nx, ny, nz, gg);
-			T gmx = qv(qg, q), gmn = qv(qg, q);
-			if (qv(q0, q) > gmx) gmx = qv(q0, q);
-			if (qv(q0, q) < gmn) gmn = qv(q0, q);
-			T d2 = T(0.0);
-			d2 += gg[0] * g0;
-			d2 += gg[1] * g1;
-			d2 += gg[2] * g2;
-			const T dmx = gmx - qv(qg, q), dmn = gmn - qv(qg, q);
-			const T lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2, dmx, dmn, T(ph.omega))
-			                                          : limiter_venkat_face(d2, dmx, dmn, eps2g);
-			T pg = T(INFINITY);
-			if (lf < pg) pg = lf;
-			v.FS[q * v.NS + ms] = recon(qv(qg, q), pg, gg[0], gg[1], gg[2], g0, g1, g2);
+#pragma unroll
+	E3D_SLOTS(k, sr) {
+		Q5<T> fs;
+		for (int q = 0; q < 5; q++)
+			qv(fs, q) = recon(qv(q0, q), phi[q], gr[q][0], gr[q][1], gr[q][2], rv[k][0], rv[k][1], rv[k][2]);
+		st5(v.FS, v.NS, sr.s0 + k, fs);
+	}
+	// ghost cells of this cell's boundary faces: gradient (reflected or zero),
+	// limiter (the ghost's only neighbour is c) and face state
+#pragma unroll
+	E3D_SLOTS(k, sr) {
+		if (nb[k] >= v.NR) {
+			const int g = nb[k];
+			int ms = v.slot_mate[sr.s0 + k];
+			ms = ms >= 0 ? ms : ~ms;
+			const Q5<T> qg = ld5(v.Pin, v.NA, g);
+			const T nx = v.sgeo[4 * (size_t)(sr.s0 + k)], ny = v.sgeo[4 * (size_t)(sr.s0 + k) + 1],
+			        nz = v.sgeo[4 * (size_t)(sr.s0 + k) + 2];
+			const T g0 = v.srv[3 * (size_t)ms], g1 = v.srv[3 * (size_t)ms + 1], g2 = v.srv[3 * (size_t)ms + 2];
+			const bool refl = v.grefl[g - v.NR] != 0;
+			const T eps2g = T(ph.k3) * v.vol[g];
+			Q5<T> fs;
+			for (int q = 0; q < 5; q++) {
+				T gg[3] = {T(0.0), T(0.0), T(0.0)};
+				if (refl) reflect_grad(gr[q], nx, ny, nz, gg);
+				T gmx = qv(qg, q), gmn = qv(qg, q);
+				if (qv(q0, q) > gmx) gmx = qv(q0, q);
+				if (qv(q0, q) < gmn) gmn = qv(q0, q);
+				T d2 = T(0.0);
+				d2 += gg[0] * g0;
+				d2 += gg[1] * g1;
+				d2 += gg[2] * g2;
+				const T dmx = gmx - qv(qg, q), dmn = gmn - qv(qg, q);
+				const T lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2, dmx, dmn, T(ph.omega))
+				                                          : limiter_venkat_face(d2, dmx, dmn, eps2g);
+				T pg = T(INFINITY);
+				if (lf < pg) pg = lf;
+				qv(fs, q) = recon(qv(qg, q), pg, gg[0], gg[1], gg[2], g0, g1, g2);
+			}
+			st5(v.FS, v.NS, ms, fs);
 		}
 	}
 	if (FIRST) {
@@ -419,23 +517,22 @@ __global__ void __launch_bounds__(128) k_recon(FusedView<T> v, Physics ph, int c
 			v.W0[4 * n + c] = (double)(T(0.5) * q0.r * (q0.u * q0.u + q0.v * q0.v + q0.w * q0.w) +
 			                           T(1.) / (T(ph.gamma) - T(1.0)) * q0.p);
 		}
+		T geo[MAXSL][4];
+		load_geo<T, NSL>(v.sgeo, sr, geo);
 		const T cc = tsqrt(T(ph.gamma) * q0.p / q0.r);
-		T sr = T(0.0);
-		for (int k = s0; k < s1; k++) {
-			const T nx = v.sgeo[4 * k], ny = v.sgeo[4 * k + 1], nz = v.sgeo[4 * k + 2], ds = v.sgeo[4 * k + 3];
-			sr += (tabs((q0.u) * nx + (q0.v) * ny + (q0.w) * nz) + (cc)) * ds;
-		}
-		v.dt[c] = T(ph.cfl) * V / sr;
+		T srad = T(0.0);
+#pragma unroll
+		E3D_SLOTS(k, sr) srad += (tabs((q0.u) * geo[k][0] + (q0.v) * geo[k][1] + (q0.w) * geo[k][2]) + (cc)) * geo[k][3];
+		v.dt[c] = T(ph.cfl) * V / srad;
 	}
 }
 
 // W0 and the local time step without a reconstruction pass (first order).
-template <class T>
+template <class T, int NSL>
 __global__ void __launch_bounds__(128) k_start(FusedView<T> v, Physics ph, int carry_w0) {
 	const int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= v.NR) return;
-	const int s0 = v.tet4 ? 4 * c : v.slot_ptr[c];
-	const int s1 = v.tet4 ? s0 + 4 : v.slot_ptr[c + 1];
+	const SlotRange<T, NSL> sr(v, c);
 	const Q5<T> q0 = ld5(v.Pin, v.NA, c);
 	if (!carry_w0) {
 		const int n = v.NR;
@@ -446,13 +543,13 @@ __global__ void __launch_bounds__(128) k_start(FusedView<T> v, Physics ph, int c
 		v.W0[4 * n + c] = (double)(T(0.5) * q0.r * (q0.u * q0.u + q0.v * q0.v + q0.w * q0.w) +
 		                           T(1.) / (T(ph.gamma) - T(1.0)) * q0.p);
 	}
+	T geo[MAXSL][4];
+	load_geo<T, NSL>(v.sgeo, sr, geo);
 	const T cc = tsqrt(T(ph.gamma) * q0.p / q0.r);
-	T sr = T(0.0);
-	for (int k = s0; k < s1; k++) {
-		const T nx = v.sgeo[4 * k], ny = v.sgeo[4 * k + 1], nz = v.sgeo[4 * k + 2], ds = v.sgeo[4 * k + 3];
-		sr += (tabs((q0.u) * nx + (q0.v) * ny + (q0.w) * nz) + (cc)) * ds;
-	}
-	v.dt[c] = T(ph.cfl) * v.vol[c] / sr;
+	T srad = T(0.0);
+#pragma unroll
+	E3D_SLOTS(k, sr) srad += (tabs((q0.u) * geo[k][0] + (q0.v) * geo[k][1] + (q0.w) * geo[k][2]) + (cc)) * geo[k][3];
+	v.dt[c] = T(ph.cfl) * v.vol[c] / srad;
 }
 
 // Pass 2 of a stage, one thread per real cell: convective and dissipative
@@ -460,42 +557,51 @@ __global__ void __launch_bounds__(128) k_start(FusedView<T> v, Physics ph, int c
 // conservative update into Pout and the ghost states of the cell's boundary
 // faces.  ORDER1 reads cell states directly (first order).  LAST stores the
 // final conservative state as the next W0 when carry_w0 is set.
-template <class T, int SCHEME, bool ORDER1>
-__global__ void __launch_bounds__(128) k_flux_update(FusedView<T> v, Physics ph, T alpha, T beta, int last, int carry_w0) {
+template <class T, int SCHEME, bool ORDER1, int NSL>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update(FusedView<T> v, Physics ph, T alpha, T beta, int last, int carry_w0) {
 	const int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= v.NR) return;
-	const int s0 = v.tet4 ? 4 * c : v.slot_ptr[c];
-	const int s1 = v.tet4 ? s0 + 4 : v.slot_ptr[c + 1];
+	const SlotRange<T, NSL> sr(v, c);
 	const T g = T(ph.gamma), gr = T(ph.gr), gm1 = T(ph.gm1);
+	int mate[MAXSL];
+	load_int<T, NSL>(v.slot_mate, sr, mate);
 	T ac[5], ad[5];
 	for (int q = 0; q < 5; q++) {
 		ac[q] = T(0.0);
 		ad[q] = v.Rd[q * v.NR + c] * (T(1.0) - beta);
 	}
 	Q5<T> qc;
-	if (ORDER1) qc = ld5(v.Pin, v.NA, c);
-	for (int k = s0; k < s1; k++) {
-		int m = v.slot_mate[k];
-		const bool left = m >= 0;
-		if (!left) m = ~m;
+	int nb[MAXSL];
+	if (ORDER1) {
+		qc = ld5(v.Pin, v.NA, c);
+		load_int<T, NSL>(v.slot_nbr, sr, nb);
+	}
+	T geo[MAXSL][4];
+	load_geo<T, NSL>(v.sgeo, sr, geo);
+#pragma unroll
+	E3D_SLOTS(k, sr) {
+		const bool left = mate[k] >= 0;
+		const int m = left ? mate[k] : ~mate[k];
 		Q5<T> qo, qn;
 		if (ORDER1) {
 			qo = qc;
-			qn = ld5(v.Pin, v.NA, v.slot_nbr[k]);
+			qn = ld5(v.Pin, v.NA, nb[k]);
 		} else {
-			qo = ld5(v.FS, v.NS, k);
+			qo = ld5(v.FS, v.NS, sr.s0 + k);
 			qn = ld5(v.FS, v.NS, m);
 		}
-		const Q5<T>& L = left ? qo : qn;
-		const Q5<T>& R = left ? qn : qo;
-		const T nx = v.sgeo[4 * k], ny = v.sgeo[4 * k + 1], nz = v.sgeo[4 * k + 2], nn = v.sgeo[4 * k + 3];
+		Q5<T> L, R;
+		for (int q = 0; q < 5; q++) {
+			qv(L, q) = left ? qv(qo, q) : qv(qn, q);
+			qv(R, q) = left ? qv(qn, q) : qv(qo, q);
+		}
 		T fc[5], fd[5];
 		if (SCHEME == FLUX_ROE) {
-			flux_central(L, R, nx, ny, nz, nn, gr, fc);
-			flux_roe_diss(L, R, nx, ny, nz, nn, gr, gm1, fd);
+			flux_central(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], gr, fc);
+			flux_roe_diss(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], gr, gm1, fd);
 		} else {
-			flux_ausm_conv(L, R, nx, ny, nz, nn, g, gr, fc);
-			flux_ausm_diss(L, R, nx, ny, nz, nn, g, gr, fd);
+			flux_ausm_conv(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], g, gr, fc);
+			flux_ausm_diss(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], g, gr, fd);
 		}
 		if (left) {
 			for (int q = 0; q < 5; q++) {
@@ -520,19 +626,19 @@ __global__ void __launch_bounds__(128) k_flux_update(FusedView<T> v, Physics ph,
 	st5(v.Pout, v.NA, c, qnew);
 	if (last && carry_w0)
 		for (int q = 0; q < 5; q++) v.W0[q * v.NR + c] = wn[q];
+	if (!ORDER1) load_int<T, NSL>(v.slot_nbr, sr, nb);
 	Q5<T> fr;
 	fr.r = T(ph.free[0]);
 	fr.u = T(ph.free[1]);
 	fr.v = T(ph.free[2]);
 	fr.w = T(ph.free[3]);
 	fr.p = T(ph.free[4]);
-	for (int k = s0; k < s1; k++) {
-		const int nb = v.slot_nbr[k];
-		if (nb < v.NR) continue;
-		const int kind = v.gkind[nb - v.NR];
-		if (kind == GK_NONE) continue;
-		const Q5<T> qg = ghost_state(kind, qnew, fr, v.sgeo[4 * k], v.sgeo[4 * k + 1], v.sgeo[4 * k + 2], g);
-		st5(v.Pout, v.NA, nb, qg);
+#pragma unroll
+	E3D_SLOTS(k, sr) {
+		if (nb[k] >= v.NR) {
+			const int kind = v.gkind[nb[k] - v.NR];
+			if (kind != GK_NONE) st5(v.Pout, v.NA, nb[k], ghost_state(kind, qnew, fr, geo[k][0], geo[k][1], geo[k][2], g));
+		}
 	}
 }
 
@@ -577,36 +683,51 @@ __global__ void k_norm_final(const double* __restrict__ partial, int nblocks, in
 	if (!isfinite(s)) *bad = 1;
 }
 
-// Wall pressure force sums per block, sequential in wall-face order like
-// AerodynamicParameters::computeAerodynamic (AerodynamicParameters.cpp:189-232).
-// hist[iter*stride + b*10 + 5 + {0..4}] = sum fy, sum fx, cmx, cmy, cmz.
+// Wall pressure forces (AerodynamicParameters::computeAerodynamic,
+// AerodynamicParameters.cpp:189-232) in two passes that keep the reference's
+// sequential wall-face order: per-face terms in parallel, then one ordered sum
+// per block and component from shared memory.
+// terms[q*nwall + i], q = fy, fx, cmx, cmy, cmz of wall face i.
 template <class T>
-__global__ void k_forces(const T* __restrict__ P, int NA, const int* __restrict__ wall_off,
-                         const int* __restrict__ wall_face, const int* __restrict__ face_lr,
-                         const double* __restrict__ S, const double* __restrict__ fc, double denom, int nblocks,
-                         double* __restrict__ hist, int stride, const int* __restrict__ d_iter) {
-	const int b = blockIdx.x * blockDim.x + threadIdx.x;
-	if (b >= nblocks) return;
-	double cl = 0., cd = 0., cmx = 0., cmy = 0., cmz = 0.;
-	for (int i = wall_off[b]; i < wall_off[b + 1]; i++) {
-		const int f = wall_face[i];
-		const double p0 = (double)P[4 * NA + face_lr[2 * f]], p1 = (double)P[4 * NA + face_lr[2 * f + 1]];
-		const double pbc = 0.5 * (p0 + p1);
-		const double cp = (pbc - 1.) / denom;
-		const double fx = cp * S[3 * f], fy = cp * S[3 * f + 1], fz = cp * S[3 * f + 2];
-		const double x = fc[3 * f], y = fc[3 * f + 1], z = fc[3 * f + 2];
-		cl += fy;
-		cd += fx;
-		cmx += y * fz - z * fy;
-		cmy += z * fx - x * fz;
-		cmz += x * fy - y * fx;
+__global__ void k_wall_terms(const T* __restrict__ P, int NA, int nwall, const int* __restrict__ wall_face,
+                             const int* __restrict__ face_lr, const double* __restrict__ S,
+                             const double* __restrict__ fc, double denom, double* __restrict__ terms) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nwall) return;
+	const int f = wall_face[i];
+	const double p0 = (double)P[4 * (size_t)NA + face_lr[2 * f]], p1 = (double)P[4 * (size_t)NA + face_lr[2 * f + 1]];
+	const double pbc = 0.5 * (p0 + p1);
+	const double cp = (pbc - 1.) / denom;
+	const double fx = cp * S[3 * f], fy = cp * S[3 * f + 1], fz = cp * S[3 * f + 2];
+	const double x = fc[3 * f], y = fc[3 * f + 1], z = fc[3 * f + 2];
+	terms[i] = fy;
+	terms[(size_t)nwall + i] = fx;
+	terms[2 * (size_t)nwall + i] = y * fz - z * fy;
+	terms[3 * (size_t)nwall + i] = z * fx - x * fz;
+	terms[4 * (size_t)nwall + i] = x * fy - y * fx;
+}
+
+// hist[iter*stride + b*10 + 5 + q] = sum of terms q over block b's wall faces, in order.
+constexpr int WALL_CHUNK = 1024;
+__global__ void __launch_bounds__(128) k_wall_sums(const double* __restrict__ terms, int nwall,
+                                                   const int* __restrict__ wall_off, double* __restrict__ hist,
+                                                   int stride, const int* __restrict__ d_iter) {
+	__shared__ double buf[5][WALL_CHUNK];
+	const int b = blockIdx.x;
+	const int beg = wall_off[b], end = wall_off[b + 1];
+	double acc = 0.;
+	for (int base = beg; base < end; base += WALL_CHUNK) {
+		const int n = min(WALL_CHUNK, end - base);
+		for (int j = threadIdx.x; j < 5 * n; j += blockDim.x) {
+			const int q = j / n, i = j - q * n;
+			buf[q][i] = terms[(size_t)q * nwall + base + i];
+		}
+		__syncthreads();
+		if (threadIdx.x < 5)
+			for (int i = 0; i < n; i++) acc += buf[threadIdx.x][i];
+		__syncthreads();
 	}
-	double* out = hist + (size_t)(*d_iter) * stride + b * 10 + 5;
-	out[0] = cl;
-	out[1] = cd;
-	out[2] = cmx;
-	out[3] = cmy;
-	out[4] = cmz;
+	if (threadIdx.x < 5) hist[(size_t)(*d_iter) * stride + b * 10 + 5 + threadIdx.x] = acc;
 }
 
 __global__ void k_iter_advance(int* d_iter) { *d_iter += 1; }

@@ -34,6 +34,8 @@ struct ReduceArgs {
 	double* partial;       // nblocks*max_chunks*5
 	const int* wall_off;   // nblocks+1
 	const int* wall_face;
+	int n_wall;
+	double* wall_terms;    // 5*n_wall
 	const int* face_lr;
 	const double* S;
 	const double* fc;
@@ -52,6 +54,7 @@ template <class T>
 void launch_recon(const FusedView<T>&, const Physics&, int grad, int lim, bool first, int carry, cudaStream_t);
 template <class T>
 void launch_start(const FusedView<T>&, const Physics&, int carry, cudaStream_t);
+
 template <class T>
 void launch_flux_update(const FusedView<T>&, const Physics&, int scheme, bool order1, double alpha, double beta,
                         int last, int carry, cudaStream_t);

@@ -17,15 +17,22 @@ void launch_reduce(const ReduceArgs& a, const T* Rc, const T* Rd, const T* P, cu
 	k_norm_partial<T, THREADS><<<grid, THREADS, 0, st>>>(Rc, Rd, a.NR, a.roff, a.chunk, a.max_chunks, a.partial);
 	k_norm_final<<<(a.nblocks * 5 + 127) / 128, 128, 0, st>>>(a.partial, a.nblocks, a.max_chunks, a.hist, a.stride,
 	                                                         a.d_iter, a.d_bad);
-	k_forces<T><<<(a.nblocks + 63) / 64, 64, 0, st>>>(P, a.NA, a.wall_off, a.wall_face, a.face_lr, a.S, a.fc, a.denom,
-	                                                  a.nblocks, a.hist, a.stride, a.d_iter);
+	if (a.n_wall > 0)
+		k_wall_terms<T><<<(a.n_wall + 127) / 128, 128, 0, st>>>(P, a.NA, a.n_wall, a.wall_face, a.face_lr, a.S, a.fc,
+		                                                     a.denom, a.wall_terms);
+	k_wall_sums<<<a.nblocks, 128, 0, st>>>(a.wall_terms, a.n_wall, a.wall_off, a.hist, a.stride, a.d_iter);
 }
 
 template <class T, int GRAD, int LIM>
 void recon_dispatch_first(const FusedView<T>& v, const Physics& ph, bool first, int carry, cudaStream_t st) {
 	const int grid = (v.NR + 127) / 128;
-	if (first) k_recon<T, GRAD, LIM, true><<<grid, 128, 0, st>>>(v, ph, carry);
-	else k_recon<T, GRAD, LIM, false><<<grid, 128, 0, st>>>(v, ph, carry);
+	if (v.tet4) {
+		if (first) k_recon<T, GRAD, LIM, true, 4><<<grid, 128, 0, st>>>(v, ph, carry);
+		else k_recon<T, GRAD, LIM, false, 4><<<grid, 128, 0, st>>>(v, ph, carry);
+	} else {
+		if (first) k_recon<T, GRAD, LIM, true, 0><<<grid, 128, 0, st>>>(v, ph, carry);
+		else k_recon<T, GRAD, LIM, false, 0><<<grid, 128, 0, st>>>(v, ph, carry);
+	}
 }
 
 template <class T>
@@ -46,7 +53,9 @@ void launch_recon(const FusedView<T>& v, const Physics& ph, int grad, int lim, b
 
 template <class T>
 void launch_start(const FusedView<T>& v, const Physics& ph, int carry, cudaStream_t st) {
-	if (v.NR > 0) k_start<T><<<(v.NR + 127) / 128, 128, 0, st>>>(v, ph, carry);
+	if (v.NR <= 0) return;
+	if (v.tet4) k_start<T, 4><<<(v.NR + 127) / 128, 128, 0, st>>>(v, ph, carry);
+	else k_start<T, 0><<<(v.NR + 127) / 128, 128, 0, st>>>(v, ph, carry);
 }
 
 template <class T>
@@ -55,13 +64,19 @@ void launch_flux_update(const FusedView<T>& v, const Physics& ph, int scheme, bo
 	if (v.NR <= 0) return;
 	const int grid = (v.NR + 127) / 128;
 	const T a = T(alpha), b = T(beta);
+#define E3D_FLUX(S, O)                                                                                  \
+	do {                                                                                                \
+		if (v.tet4) k_flux_update<T, S, O, 4><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);          \
+		else k_flux_update<T, S, O, 0><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);                 \
+	} while (0)
 	if (scheme == FLUX_AUSM) {
-		if (order1) k_flux_update<T, FLUX_AUSM, true><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);
-		else k_flux_update<T, FLUX_AUSM, false><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);
+		if (order1) E3D_FLUX(FLUX_AUSM, true);
+		else E3D_FLUX(FLUX_AUSM, false);
 	} else {
-		if (order1) k_flux_update<T, FLUX_ROE, true><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);
-		else k_flux_update<T, FLUX_ROE, false><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);
+		if (order1) E3D_FLUX(FLUX_ROE, true);
+		else E3D_FLUX(FLUX_ROE, false);
 	}
+#undef E3D_FLUX
 }
 
 }  // namespace e3d
