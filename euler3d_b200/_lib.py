@@ -95,6 +95,8 @@ SIGNATURES = {
     "e3d_time_kernels": ([C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                           C.POINTER(C.c_int)], C.c_int),
     "e3d_launches_per_iteration": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "e3d_residual_norms_noalloc": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                    C.c_void_p], C.c_int),
 }
 
 

@@ -50,6 +50,10 @@ e3d::Engine& eng(e3d_solver* s) {
 }
 }  // namespace
 
+namespace e3d {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace e3d
+
 extern "C" {
 
 const char* e3d_last_error(void) { return g_err.c_str(); }

@@ -159,6 +159,29 @@ int e3d_state_bytes(const e3d_solver* s, int64_t* bytes);
 int e3d_state_export(e3d_solver* s, void* host, int64_t bytes);
 int e3d_state_import(e3d_solver* s, const void* host, int64_t bytes);
 
+/* ---- residual norms without device allocation ---------------------------------
+ * No counterpart in the reference (its norms are host loops).  For callers that
+ * cannot allocate device memory where they need the norms: a host application
+ * that owns all device memory through its own pool and forbids cudaMalloc in
+ * plugins, or a time-stepping loop that must not allocate.  Computes, like
+ * e3d_flow_data's out[b*10 + 0..4], the per-block sums of (rc - rd)^2 per
+ * equation, with its scratch in a static device array of
+ * E3D_NOALLOC_MAX_PARTIALS x 5 doubles (320 KiB, held by every GPU that loads
+ * the library until exit) instead of cudaMalloc.
+ *   rc, rd         device [5][n_cells] FP64 residuals, equation-major
+ *   block_offsets  device [n_blocks+1]: block b owns cells [off[b], off[b+1])
+ *   max_block_cells  largest block size; n_blocks * ceil(max_block_cells/4096)
+ *                  must not exceed E3D_NOALLOC_MAX_PARTIALS (else E3D_ERR_LIMIT)
+ *   out            device [n_blocks*5]
+ *   stream         cudaStream_t or NULL
+ * Queued on `stream`, nothing is allocated or freed.  The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress): make it before
+ * any stream capture.  Calls share the scratch, so calls that overlap on the
+ * GPU race; order them on one stream. */
+#define E3D_NOALLOC_MAX_PARTIALS 8192
+int e3d_residual_norms_noalloc(const double* rc, const double* rd, int64_t n_cells, int n_blocks,
+                               const int32_t* block_offsets, int max_block_cells, double* out, void* stream);
+
 /* Measurement: per-kernel CUDA-event times of n eager iterations on the solver
  * stream.  names: comma-separated kernel names; launches/total_ms/bytes per row. */
 int e3d_time_kernels(e3d_solver* s, int n_iter, char* names, int names_len, int* launches, double* total_ms,
