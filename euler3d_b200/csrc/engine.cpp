@@ -972,18 +972,19 @@ double Engine::bytes_start() const {
 	const double NSR = tet4_ ? 4.0 * NR_ : (double)NS_ - NG_;
 	return 5 * b * NR_ + 4 * b * NSR + b * NR_ + 5 * 8.0 * (carry_ ? 0 : NR_) + b * NR_;
 }
-double Engine::bytes_flux(bool order1) const {
+double Engine::bytes_flux(bool order1, bool diss, bool last) const {
 	const double b = opt_.precision == PREC_FP64 ? 8.0 : 4.0;
 	const double NSR = tet4_ ? 4.0 * NR_ : (double)NS_ - NG_;
 	double x = 4.0 * NSR + 4.0 * NSR       // mate and neighbour ids
 	           + 4 * b * NSR               // face normal and area
-	           + 5 * b * NR_ * 2           // Rd read, Rc written
-	           + 5 * b * NR_               // Rd written
+	           + 5 * b * NR_               // Rd read
 	           + 5 * 8.0 * NR_             // W0 read
 	           + 2 * b * NR_               // dt, volume
 	           + 5 * b * NA_               // new cell and ghost states written
 	           + 1.0 * NG_;                // ghost kinds
 	x += order1 ? 5 * b * NA_ : 5 * b * NS_;  // cell states or face states read
+	if (diss) x += 5 * b * NR_;               // Rd written
+	if (last) x += 5 * b * NR_ + (carry_ ? 5 * 8.0 * NR_ : 0.0);  // Rc (and carried W) written
 	return x;
 }
 
@@ -1001,8 +1002,9 @@ std::vector<Engine::KernelTime> Engine::time_kernels(int n) {
 			names.push_back("start");
 			bytes.push_back(bytes_start());
 		}
-		names.push_back("flux_update");
-		bytes.push_back(bytes_flux(order_ == 1));
+		const bool diss = beta_[s] != 0.0, last = s == stages - 1;
+		names.push_back(last ? "flux_update_last" : diss ? "flux_update" : "flux_update_nodiss");
+		bytes.push_back(bytes_flux(order_ == 1, diss, last));
 	}
 	names.push_back("reduce_halo");
 	bytes.push_back(0.0);

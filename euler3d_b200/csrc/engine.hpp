@@ -93,7 +93,7 @@ public:
 	// algorithmic bytes (distinct elements touched) of one launch of each fused kernel
 	double bytes_recon(bool first) const;
 	double bytes_start() const;
-	double bytes_flux(bool order1) const;
+	double bytes_flux(bool order1, bool diss, bool last) const;
 	// times each fused kernel of `n` eager (un-captured) iterations with CUDA events on
 	// the engine stream; returns {name, launches, total_ms}
 	struct KernelTime {

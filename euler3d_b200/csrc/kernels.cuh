@@ -449,28 +449,51 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_recon(FusedView
 			for (int q = 0; q < 5; q++) gr[q][d] /= V;
 	T rv[MAXSL][3];
 	load3<T, NSL>(v.srv, sr, rv);
-	T phi[5];
 	const T eps2 = T(ph.k3) * V;
-	for (int q = 0; q < 5; q++) {
-		const T dmax = qv(mx, q) - qv(q0, q), dmin = qv(mn, q) - qv(q0, q);
-		phi[q] = T(INFINITY);
+	if constexpr (sizeof(T) == 4 && NSL == 4) {
+		// FP32: the face value q + phi (g.r) reuses the limiter's d2 = g.r
+		Q5<T> fs[4];
+		for (int q = 0; q < 5; q++) {
+			const T dmax = qv(mx, q) - qv(q0, q), dmin = qv(mn, q) - qv(q0, q);
+			T d2[4], phi = T(INFINITY);
+#pragma unroll
+			for (int k = 0; k < 4; k++) {
+				d2[k] = gr[q][0] * rv[k][0];
+				d2[k] += gr[q][1] * rv[k][1];
+				d2[k] += gr[q][2] * rv[k][2];
+				const T lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2[k], dmax, dmin, T(ph.omega))
+				                                          : limiter_venkat_face(d2[k], dmax, dmin, eps2);
+				if (lf < phi) phi = lf;
+			}
+#pragma unroll
+			for (int k = 0; k < 4; k++) qv(fs[k], q) = qv(q0, q) + phi * d2[k];
+		}
+#pragma unroll
+		for (int k = 0; k < 4; k++) st5(v.FS, v.NS, sr.s0 + k, fs[k]);
+	} else {
+		// FP64 (and the generic slot path): the reference's accumulation order
+		T phi[5];
+		for (int q = 0; q < 5; q++) {
+			const T dmax = qv(mx, q) - qv(q0, q), dmin = qv(mn, q) - qv(q0, q);
+			phi[q] = T(INFINITY);
+#pragma unroll
+			E3D_SLOTS(k, sr) {
+				T d2 = T(0.0);
+				d2 += gr[q][0] * rv[k][0];
+				d2 += gr[q][1] * rv[k][1];
+				d2 += gr[q][2] * rv[k][2];
+				const T lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2, dmax, dmin, T(ph.omega))
+				                                          : limiter_venkat_face(d2, dmax, dmin, eps2);
+				if (lf < phi[q]) phi[q] = lf;
+			}
+		}
 #pragma unroll
 		E3D_SLOTS(k, sr) {
-			T d2 = T(0.0);
-			d2 += gr[q][0] * rv[k][0];
-			d2 += gr[q][1] * rv[k][1];
-			d2 += gr[q][2] * rv[k][2];
-			const T lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2, dmax, dmin, T(ph.omega))
-			                                          : limiter_venkat_face(d2, dmax, dmin, eps2);
-			if (lf < phi[q]) phi[q] = lf;
+			Q5<T> fs;
+			for (int q = 0; q < 5; q++)
+				qv(fs, q) = recon(qv(q0, q), phi[q], gr[q][0], gr[q][1], gr[q][2], rv[k][0], rv[k][1], rv[k][2]);
+			st5(v.FS, v.NS, sr.s0 + k, fs);
 		}
-	}
-#pragma unroll
-	E3D_SLOTS(k, sr) {
-		Q5<T> fs;
-		for (int q = 0; q < 5; q++)
-			qv(fs, q) = recon(qv(q0, q), phi[q], gr[q][0], gr[q][1], gr[q][2], rv[k][0], rv[k][1], rv[k][2]);
-		st5(v.FS, v.NS, sr.s0 + k, fs);
 	}
 	// ghost cells of this cell's boundary faces: gradient (reflected or zero),
 	// limiter (the ghost's only neighbour is c) and face state
@@ -557,7 +580,12 @@ __global__ void __launch_bounds__(128) k_start(FusedView<T> v, Physics ph, int c
 // conservative update into Pout and the ghost states of the cell's boundary
 // faces.  ORDER1 reads cell states directly (first order).  LAST stores the
 // final conservative state as the next W0 when carry_w0 is set.
-template <class T, int SCHEME, bool ORDER1, int NSL>
+//
+// DISS = false is used for stages with beta = 0: the reference still evaluates
+// the dissipative flux (its guard is always true) but Rd*(1-0) + sum(D*0) equals
+// Rd for finite fluxes, so the flux and the Rd store are skipped.  Rc is stored
+// only at the last stage, the one the norms (and callers) read.
+template <class T, int SCHEME, bool ORDER1, int NSL, bool DISS>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update(FusedView<T> v, Physics ph, T alpha, T beta, int last, int carry_w0) {
 	const int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= v.NR) return;
@@ -568,7 +596,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update(Fus
 	T ac[5], ad[5];
 	for (int q = 0; q < 5; q++) {
 		ac[q] = T(0.0);
-		ad[q] = v.Rd[q * v.NR + c] * (T(1.0) - beta);
+		ad[q] = DISS ? v.Rd[q * v.NR + c] * (T(1.0) - beta) : v.Rd[q * v.NR + c];
 	}
 	Q5<T> qc;
 	int nb[MAXSL];
@@ -598,27 +626,27 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update(Fus
 		T fc[5], fd[5];
 		if (SCHEME == FLUX_ROE) {
 			flux_central(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], gr, fc);
-			flux_roe_diss(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], gr, gm1, fd);
+			if (DISS) flux_roe_diss(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], gr, gm1, fd);
 		} else {
 			flux_ausm_conv(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], g, gr, fc);
-			flux_ausm_diss(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], g, gr, fd);
+			if (DISS) flux_ausm_diss(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], g, gr, fd);
 		}
 		if (left) {
 			for (int q = 0; q < 5; q++) {
 				ac[q] += fc[q];
-				ad[q] += fd[q] * beta;
+				if (DISS) ad[q] += fd[q] * beta;
 			}
 		} else {
 			for (int q = 0; q < 5; q++) {
 				ac[q] -= fc[q];
-				ad[q] -= fd[q] * beta;
+				if (DISS) ad[q] -= fd[q] * beta;
 			}
 		}
 	}
 	double w0[5], wn[5];
 	for (int q = 0; q < 5; q++) {
-		v.Rc[q * v.NR + c] = ac[q];
-		v.Rd[q * v.NR + c] = ad[q];
+		if (last) v.Rc[q * v.NR + c] = ac[q];
+		if (DISS) v.Rd[q * v.NR + c] = ad[q];
 		w0[q] = v.W0[q * v.NR + c];
 	}
 	const T coef = alpha * v.dt[c] / v.vol[c];

@@ -66,8 +66,13 @@ void launch_flux_update(const FusedView<T>& v, const Physics& ph, int scheme, bo
 	const T a = T(alpha), b = T(beta);
 #define E3D_FLUX(S, O)                                                                                  \
 	do {                                                                                                \
-		if (v.tet4) k_flux_update<T, S, O, 4><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);          \
-		else k_flux_update<T, S, O, 0><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);                 \
+		if (beta != 0.0) {                                                                              \
+			if (v.tet4) k_flux_update<T, S, O, 4, true><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);  \
+			else k_flux_update<T, S, O, 0, true><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);         \
+		} else {                                                                                        \
+			if (v.tet4) k_flux_update<T, S, O, 4, false><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry); \
+			else k_flux_update<T, S, O, 0, false><<<grid, 128, 0, st>>>(v, ph, a, b, last, carry);        \
+		}                                                                                               \
 	} while (0)
 	if (scheme == FLUX_AUSM) {
 		if (order1) E3D_FLUX(FLUX_AUSM, true);

@@ -207,15 +207,27 @@ __device__ __forceinline__ T limiter_bj_face(T d2, T dmax, T dmin, T omega) {
 }
 
 // Venkatakrishnan face limiter, eps2 = K^3 * V (Venkatakrishnan.cpp:92,227-238).
+// The double version keeps the reference's expression (two divisions); the
+// float version uses the same function with d2 cancelled from numerator and
+// denominator, (D^2+eps2+2 d2 D) / (D^2+eps2 + d2 (2 d2 + D)), one division.
 template <class T>
-__device__ __forceinline__ T limiter_venkat_face(T d2, T dmax, T dmin, T eps2) {
-	if (d2 > T(0.0))
-		return (T(1.0) / d2) * ((dmax * dmax + eps2) * d2 + T(2.0) * d2 * d2 * dmax) /
-		       (dmax * dmax + T(2.0) * d2 * d2 + dmax * d2 + eps2);
-	if (d2 < T(0.0))
-		return (T(1.0) / d2) * ((dmin * dmin + eps2) * d2 + T(2.0) * d2 * d2 * dmin) /
-		       (dmin * dmin + T(2.0) * d2 * d2 + dmin * d2 + eps2);
-	return T(1.0);
+__device__ __forceinline__ T limiter_venkat_face(T d2, T dmax, T dmin, T eps2);
+template <>
+__device__ __forceinline__ float limiter_venkat_face<float>(float d2, float dmax, float dmin, float eps2) {
+	if (!(d2 > 0.0f) && !(d2 < 0.0f)) return 1.0f;  // zero or NaN, as the reference's branches
+	const float D = d2 > 0.0f ? dmax : dmin;
+	const float A = fmaf(D, D, eps2);
+	return fmaf(2.0f * d2, D, A) / fmaf(d2, fmaf(2.0f, d2, D), A);
+}
+template <>
+__device__ __forceinline__ double limiter_venkat_face<double>(double d2, double dmax, double dmin, double eps2) {
+	if (d2 > double(0.0))
+		return (double(1.0) / d2) * ((dmax * dmax + eps2) * d2 + double(2.0) * d2 * d2 * dmax) /
+		       (dmax * dmax + double(2.0) * d2 * d2 + dmax * d2 + eps2);
+	if (d2 < double(0.0))
+		return (double(1.0) / d2) * ((dmin * dmin + eps2) * d2 + double(2.0) * d2 * d2 * dmin) /
+		       (dmin * dmin + double(2.0) * d2 * d2 + dmin * d2 + eps2);
+	return double(1.0);
 }
 
 // Slip wall / symmetry ghost state (WallCellIds.cpp:40-62, SymmetryCellIds.cpp:41-63).
