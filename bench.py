@@ -204,6 +204,20 @@ def run_reference_arm(a, rank: int):
     return 0
 
 
+# ------------------------------------------------------------------ ranks
+def combine_ranks(local_ms: float, cells: int, steps: int, world: int, dist=None, device="cpu") -> dict:
+    """Replicas: every rank advances its own copy of the workload; the job's
+    time is the slowest rank's device time (max over ranks), and the job
+    processed world x cells x steps cell-iterations."""
+    import torch
+
+    t = torch.tensor([local_ms], dtype=torch.float64, device=device)
+    if world > 1 and dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    return {"ms": ms, "value": world * cells * steps / (ms / 1000.0)}
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -257,13 +271,10 @@ def main():
         ms = s.iterate_timed(steps)  # CUDA events on the solver stream around the K graph launches
         clocks.mark("end")
         torch.cuda.synchronize()
-        t_ms = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
-        ms = float(t_ms.item())
+        comb = combine_ranks(ms, cells, steps, world, dist if world > 1 else None, device="cuda")
+        ms, value = comb["ms"], comb["value"]
         hist = s.history()
         assert all(abs(x) < 1e300 for x in hist["rms"][:, 0]), "non-finite residual"
-        value = world * cells * steps / (ms / 1000.0)
         launches = s.launches_per_iteration() * steps
 
         # per-kernel device times (eager launches with events between kernels)

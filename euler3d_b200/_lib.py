@@ -95,6 +95,13 @@ SIGNATURES = {
     "e3d_time_kernels": ([C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                           C.POINTER(C.c_int)], C.c_int),
     "e3d_launches_per_iteration": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "e3d_batch_create": ([C.c_void_p, C.c_int, C.POINTER(Options), C.POINTER(C.c_void_p)], C.c_int),
+    "e3d_batch_solve": ([C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_void_p, C.POINTER(C.c_double)], C.c_int),
+    "e3d_case_count": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "e3d_case_history_length": ([C.c_void_p, C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "e3d_case_history": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
+    "e3d_batch_tuning": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
+                          C.POINTER(C.c_int)], C.c_int),
     "e3d_residual_norms_noalloc": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                     C.c_void_p], C.c_int),
 }

@@ -203,6 +203,53 @@ class Solver:
             pass
 
 
+class Batch(Solver):
+    """Several cases advanced together (one device arena, persistent kernel)."""
+
+    def __init__(self, cases: list, precision: str = "fp32", use_graph: bool = True, device: int = -1,
+                 hist_capacity: int = 4096):
+        lib = L.lib()
+        o = L.Options()
+        lib.e3d_default_options(C.byref(o))
+        o.precision = L.FP32 if precision == "fp32" else L.FP64
+        o.use_graph = 1 if use_graph else 0
+        o.device = device
+        o.hist_capacity = hist_capacity
+        arr = (C.c_void_p * len(cases))(*[c._h.value for c in cases])
+        h = C.c_void_p()
+        L.check(lib.e3d_batch_create(arr, len(cases), C.byref(o), C.byref(h)))
+        self._h = h
+        self.cases = cases
+        self.case = cases[0]
+        self.precision = precision
+        self.n_blocks = sum(c.n_blocks for c in cases)
+        self._info = [c.block_info(b) for c in cases for b in range(c.n_blocks)]
+
+    def solve_batch(self, max_iter: int, criterion: float, iters_per_launch: int = 10):
+        """Returns (iterations needed per case, device ms of the whole solve)."""
+        done = np.zeros(len(self.cases), dtype=np.int32)
+        ms = C.c_double()
+        L.check(L.lib().e3d_batch_solve(self._h, max_iter, criterion, iters_per_launch, L.ptr(done), C.byref(ms)))
+        return done, ms.value
+
+    def case_history(self, c: int) -> dict[str, np.ndarray]:
+        lib = L.lib()
+        n = C.c_int()
+        L.check(lib.e3d_case_history_length(self._h, c, C.byref(n)))
+        recs = (L.IterRecord * max(1, n.value))()
+        if n.value:
+            L.check(lib.e3d_case_history(self._h, c, 0, n.value, C.cast(recs, C.c_void_p)))
+        r = recs[:n.value]
+        return {"iter": np.array([x.iter for x in r]), "rms": np.array([list(x.rms) for x in r]).reshape(-1, 5),
+                "conv": np.array([list(x.conv) for x in r]).reshape(-1, 5), "cl": np.array([x.cl for x in r]),
+                "cd": np.array([x.cd for x in r])}
+
+    def tuning(self) -> dict:
+        t, g, ms, fc = C.c_int(), C.c_int(), C.c_double(), C.c_int()
+        L.check(L.lib().e3d_batch_tuning(self._h, C.byref(t), C.byref(g), C.byref(ms), C.byref(fc)))
+        return {"tile_cells": t.value, "grid": g.value, "ms_per_iter": ms.value, "from_cache": bool(fc.value)}
+
+
 # --------------------------------------------------------------------------------
 # Strategy classes with the reference's names.  A ``Block`` is one block of a
 # device-resident solver (the reference's Block*); methods launch one kernel.

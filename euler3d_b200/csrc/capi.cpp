@@ -210,6 +210,92 @@ int e3d_solver_create(const e3d_case* c, const e3d_options* opt, e3d_solver** ou
 	});
 }
 
+int e3d_batch_create(const e3d_case* const* cases, int n_cases, const e3d_options* opt, e3d_solver** out) {
+	if (!cases || n_cases <= 0 || !out) return fail(E3D_ERR_ARG, "null argument or no case");
+	*out = nullptr;
+	return guard([&] {
+		std::vector<const e3d::HostCase*> list;
+		for (int i = 0; i < n_cases; i++) {
+			if (!cases[i]) throw e3d::Error(E3D_ERR_ARG, "null case in batch");
+			list.push_back(&cases[i]->hc);
+		}
+		e3d_options o;
+		e3d_default_options(&o);
+		if (opt) o = *opt;
+		e3d::EngineOptions eo;
+		eo.precision = o.precision;
+		eo.carry_w0 = o.carry_w0;
+		eo.use_graph = o.use_graph;
+		eo.device = o.device;
+		eo.stream = static_cast<cudaStream_t>(o.stream);
+		eo.hist_capacity = o.hist_capacity > 0 ? (size_t)o.hist_capacity : 4096;
+		auto* s = new e3d_solver;
+		try {
+			s->eng.reset(new e3d::Engine(list, eo));
+		} catch (...) {
+			delete s;
+			throw;
+		}
+		*out = s;
+	});
+}
+
+int e3d_batch_solve(e3d_solver* s, int max_iter, double criterion, int iters_per_launch, int* iters_done,
+                    double* device_ms) {
+	return guard([&] {
+		std::vector<int> done;
+		const double ms = eng(s).solve_batch(max_iter, criterion, iters_per_launch, done);
+		if (iters_done)
+			for (size_t i = 0; i < done.size(); i++) iters_done[i] = done[i];
+		if (device_ms) *device_ms = ms;
+	});
+}
+
+int e3d_case_count(const e3d_solver* s, int* n) {
+	if (!s || !s->eng || !n) return fail(E3D_ERR_ARG, "null argument");
+	*n = s->eng->n_cases();
+	return E3D_OK;
+}
+
+int e3d_case_history_length(const e3d_solver* s, int case_index, int* n) {
+	if (!s || !s->eng || !n) return fail(E3D_ERR_ARG, "null argument");
+	if (case_index < 0 || case_index >= s->eng->n_cases()) return fail(E3D_ERR_ARG, "case index out of range");
+	*n = (int)s->eng->history(case_index).size();
+	return E3D_OK;
+}
+
+int e3d_case_history(const e3d_solver* s, int case_index, int first, int count, e3d_iter_record* out) {
+	if (!s || !s->eng || !out) return fail(E3D_ERR_ARG, "null argument");
+	if (case_index < 0 || case_index >= s->eng->n_cases()) return fail(E3D_ERR_ARG, "case index out of range");
+	const auto& h = s->eng->history(case_index);
+	if (first < 0 || count < 0 || (size_t)first + (size_t)count > h.size()) return fail(E3D_ERR_ARG, "history range");
+	for (int i = 0; i < count; i++) {
+		const e3d::IterRecord& r = h[(size_t)first + i];
+		e3d_iter_record& o = out[i];
+		o.iter = r.iter;
+		for (int q = 0; q < 5; q++) {
+			o.rms[q] = r.rms[q];
+			o.conv[q] = r.conv[q];
+		}
+		o.cl = r.cl;
+		o.cd = r.cd;
+		o.cmx = r.cmx;
+		o.cmy = r.cmy;
+		o.cmz = r.cmz;
+	}
+	return E3D_OK;
+}
+
+int e3d_batch_tuning(const e3d_solver* s, int* tile_cells, int* grid, double* ms_per_iter, int* from_cache) {
+	if (!s || !s->eng) return fail(E3D_ERR_ARG, "null argument");
+	const auto& t = s->eng->tuning();
+	if (tile_cells) *tile_cells = t.tile_cells;
+	if (grid) *grid = t.grid;
+	if (ms_per_iter) *ms_per_iter = t.ms_per_iter;
+	if (from_cache) *from_cache = t.from_cache ? 1 : 0;
+	return E3D_OK;
+}
+
 int e3d_solver_free(e3d_solver* s) {
 	delete s;
 	return E3D_OK;

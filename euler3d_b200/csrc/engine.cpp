@@ -4,7 +4,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace e3d {
 
@@ -35,6 +40,7 @@ template struct DevBuf<int>;
 template struct DevBuf<signed char>;
 template struct DevBuf<double>;
 template struct DevBuf<float>;
+template struct DevBuf<unsigned char>;
 
 template <class T>
 FusedView<T> Engine::Fused<T>::view(bool flip) const {
@@ -65,7 +71,19 @@ static void rk_tables(int stages, std::vector<double>& a, std::vector<double>& b
 	}
 }
 
-Engine::Engine(const HostCase& hc, const EngineOptions& opt) : deck_(hc.deck), opt_(opt) {
+Engine::Engine(const HostCase& hc, const EngineOptions& opt) : Engine(std::vector<const HostCase*>{&hc}, opt) {}
+
+Engine::Engine(const std::vector<const HostCase*>& cases, const EngineOptions& opt)
+    : deck_(cases.empty() ? Deck() : cases[0]->deck), opt_(opt) {
+	if (cases.empty()) throw Error(E3D_ERR_ARG, "no case");
+	for (const HostCase* c : cases) {
+		const Deck& d = c->deck;
+		if (d.gamma != deck_.gamma || d.cfl != deck_.cfl || d.stages != deck_.stages || d.flux != deck_.flux ||
+		    d.order != deck_.order || d.gradient != deck_.gradient || d.limiter != deck_.limiter ||
+		    d.omega != deck_.omega || d.k != deck_.k || d.smoothing != deck_.smoothing)
+			throw Error(E3D_ERR_ARG, "cases of a batch must share gamma, CFL, RK stages, flux, order, gradient, "
+			                         "limiter, omega and k");
+	}
 	if (opt_.precision != PREC_FP64 && opt_.precision != PREC_FP32) throw Error(E3D_ERR_ARG, "unknown precision");
 	if (opt_.device >= 0) cuda_ok(cudaSetDevice(opt_.device), "cudaSetDevice");
 	carry_ = opt_.carry_w0 >= 0 ? opt_.carry_w0 : (opt_.precision == PREC_FP32 ? 1 : 0);
@@ -99,6 +117,21 @@ Engine::Engine(const HostCase& hc, const EngineOptions& opt) : deck_(hc.deck), o
 	// AerodynamicParameters (AerodynamicParameters.cpp:22, :167, :212)
 	aoa_rad_ = deck_.aoa_deg * 4. * std::atan(1.) / 180;
 	denom_ = (0.5 * deck_.gamma * deck_.mach * deck_.mach) * deck_.cmac;
+	ncases_ = (int)cases.size();
+	for (const HostCase* c : cases) {
+		const Deck& d = c->deck;
+		const double pi = std::atan(1.0) * 4.0;
+		const double a = d.aoa_deg * pi / 180.0;
+		const double cs = std::cos(a), sn = std::sin(a);
+		const double f[5] = {1.0, d.mach * std::sqrt(d.gamma) * cs, d.mach * std::sqrt(d.gamma) * sn, 0.0, 1.0};
+		case_free_h_.insert(case_free_h_.end(), f, f + 5);
+		case_denom_.push_back((0.5 * d.gamma * d.mach * d.mach) * d.cmac);
+		case_aoa_.push_back(d.aoa_deg * 4. * std::atan(1.) / 180);
+	}
+	have_rms0_.assign(ncases_, 0);
+	rms0_.assign(ncases_, {0, 0, 0, 0, 0});
+	hist_case_.assign(ncases_, {});
+	case_active_.assign(ncases_, 1);
 
 	if (opt_.stream) {
 		st_ = opt_.stream;
@@ -106,19 +139,53 @@ Engine::Engine(const HostCase& hc, const EngineOptions& opt) : deck_(hc.deck), o
 		cuda_ok(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
 		own_stream_ = true;
 	}
-	build(hc);
+	setup(cases);
 	init_state();
+}
+
+void Engine::setup(const std::vector<const HostCase*>& cases) {
+	HostCase merged;
+	case_boff_.assign(1, 0);
+	std::vector<const HostBlock*> blocks;
+	std::vector<Connexion> conns;
+	for (const HostCase* c : cases) {
+		const int off = (int)blocks.size();
+		for (const HostBlock& b : c->blocks) blocks.push_back(&b);
+		for (Connexion k : c->topo.connexions) {
+			k.dest_block += off;
+			k.origin_block += off;
+			conns.push_back(std::move(k));
+		}
+		case_boff_.push_back((int)blocks.size());
+	}
+	build_blocks(blocks, conns);
+}
+
+long long Engine::n_real_case(int c) const {
+	return (long long)roff_[case_boff_.at(c + 1)] - roff_[case_boff_.at(c)];
 }
 
 Engine::~Engine() {
 	for (auto& g : graph_)
 		if (g) cudaGraphExecDestroy(g);
+	if (pgraph_) cudaGraphExecDestroy(pgraph_);
 	if (own_stream_ && st_) cudaStreamDestroy(st_);
 }
 
 void Engine::check(const char* what) { cuda_ok(cudaGetLastError(), what); }
 
-void Engine::build(const HostCase& hc) {
+void Engine::build_blocks(const std::vector<const HostBlock*>& blocks, const std::vector<Connexion>& conns) {
+	struct View {
+		const std::vector<const HostBlock*>& b;
+		size_t size() const { return b.size(); }
+		const HostBlock& operator[](size_t i) const { return *b[i]; }
+	};
+	struct {
+		View blocks;
+		struct {
+			const std::vector<Connexion>& connexions;
+		} topo;
+	} hc{View{blocks}, {conns}};
 	nb_ = (int)hc.blocks.size();
 	roff_.assign(nb_ + 1, 0);
 	goff_.assign(nb_ + 1, 0);
@@ -157,6 +224,11 @@ void Engine::build(const HostCase& hc) {
 	    fc(3 * (size_t)NF_), vol(NA_);
 	std::vector<int> face_slot_l(NF_, -1), face_slot_r(NF_, -1);
 	std::vector<signed char> gkind(NG_, GK_NONE), grefl(NG_, 0);
+	std::vector<int> gcase(NG_, 0);
+	std::vector<double> wall_denom;
+	block_case_.assign(nb_, 0);
+	for (int c = 0; c < ncases_; c++)
+		for (int b = case_boff_[c]; b < case_boff_[c + 1]; b++) block_case_[b] = c;
 	std::vector<int> wall_off(nb_ + 1, 0), wall_face;
 	for (int b = 0; b < nb_; b++) {
 		const HostBlock& B = hc.blocks[b];
@@ -201,8 +273,12 @@ void Engine::build(const HostCase& hc) {
 				                                                  : GK_SYMMETRY;
 			}
 		}
-		for (int f : B.wall_faces) wall_face.push_back(foff_[b] + f);
+		for (int f : B.wall_faces) {
+			wall_face.push_back(foff_[b] + f);
+			wall_denom.push_back(case_denom_[block_case_[b]]);
+		}
 		wall_off[b + 1] = (int)wall_face.size();
+		for (int g = B.n_real; g < B.n_all; g++) gcase[gid(b, g) - NR_] = block_case_[b];
 	}
 	for (int F = 0; F < NF_; F++)
 		if (face_slot_l[F] < 0 || face_slot_r[F] < 0) throw Error(E3D_ERR_MESH, "internal: face without two slots");
@@ -227,6 +303,11 @@ void Engine::build(const HostCase& hc) {
 	wall_off_.upload(wall_off);
 	wall_face_.upload(wall_face);
 	roff_d_.upload(roff_);
+	if (ncases_ > 1) {
+		case_free_d_.upload(case_free_h_);
+		gcase_d_.upload(gcase);
+		wall_denom_d_.upload(wall_denom);
+	}
 	gkind_.upload(gkind);
 	grefl_.upload(grefl);
 	S_.upload(S);
@@ -289,9 +370,15 @@ void Engine::init_state() {
 	// (PrimitiveVariables::initializeFlowField, PrimitiveVariables.cpp:58-69);
 	// residuals, W0, gradients and limiters start at zero (value-initialised arrays)
 	std::vector<double> P(5 * (size_t)NA_);  // packed: [NA] x (rho,u,v,w), then [NA] p
-	for (int c = 0; c < NA_; c++)
-		for (int q = 0; q < 4; q++) P[4 * (size_t)c + q] = ph_.free[q];
-	std::fill(P.begin() + 4 * (size_t)NA_, P.end(), ph_.free[4]);
+	auto fill_cell = [&](int cell, const double* f) {
+		for (int q = 0; q < 4; q++) P[4 * (size_t)cell + q] = f[q];
+		P[4 * (size_t)NA_ + cell] = f[4];
+	};
+	for (int b = 0; b < nb_; b++) {
+		const double* f = &case_free_h_[5 * (size_t)block_case_[b]];
+		for (int c = roff_[b]; c < roff_[b + 1]; c++) fill_cell(c, f);
+		for (int g = NR_ + goff_[b]; g < NR_ + goff_[b + 1]; g++) fill_cell(g, f);
+	}
 	std::vector<double> zR(5 * (size_t)NR_, 0.0);
 	if (opt_.precision == PREC_FP64) {
 		f64_.P0.upload(P);
@@ -316,8 +403,9 @@ void Engine::init_state() {
 	if (carry_) {
 		// W carried in FP64 from the freestream conservative state
 		std::vector<double> W(5 * (size_t)NR_);
-		const double* f = ph_.free;
 		for (int c = 0; c < NR_; c++) {
+			const int b = (int)(std::upper_bound(roff_.begin(), roff_.end(), c) - roff_.begin()) - 1;
+			const double* f = &case_free_h_[5 * (size_t)block_case_[b]];
 			W[c] = f[0];
 			W[(size_t)NR_ + c] = f[0] * f[1];
 			W[2 * (size_t)NR_ + c] = f[0] * f[2];
@@ -504,6 +592,7 @@ static ReduceArgs make_reduce(int NR, int NA, int nb, const int* roff, int chunk
 	a.S = S;
 	a.fc = fc;
 	a.denom = denom;
+	a.wall_denom = nullptr;
 	a.hist = hist;
 	a.stride = nb * 10;
 	a.d_iter = d_iter;
@@ -515,6 +604,7 @@ void Engine::flow_data(std::vector<double>& out) {
 	ReduceArgs a = make_reduce(NR_, NA_, nb_, roff_d_.p, chunk_, max_chunks_, partial_.p, wall_off_.p, wall_face_.p,
 	                           (int)wall_face_.n, wall_terms_.p, face_lr_.p, S_.p, fc_.p, denom_, fd_hist_.p, zero_d_.p,
 	                           bad_d_.p);
+	a.wall_denom = wall_denom_d_.p;
 	if (opt_.precision == PREC_FP64)
 		launch_reduce<double>(a, f64_.Rc.p, f64_.Rd.p, cur_ ? f64_.P1.p : f64_.P0.p, st_);
 	else
@@ -553,6 +643,8 @@ void Engine::iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* m
 		v.gkind = gkind_.p;
 		v.grefl = grefl_.p;
 		v.W0 = W0_.p;
+		v.case_free = case_free_d_.p;
+		v.gcase = gcase_d_.p;
 		if (order_ == 2) {
 			launch_recon<T>(v, ph_, grad_kind_, lim_kind_, s == 0, carry_, st_);
 			mark();
@@ -570,6 +662,7 @@ void Engine::iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* m
 	ReduceArgs a = make_reduce(NR_, NA_, nb_, roff_d_.p, chunk_, max_chunks_, partial_.p, wall_off_.p, wall_face_.p,
 	                           (int)wall_face_.n, wall_terms_.p, face_lr_.p, S_.p, fc_.p, denom_, hist_d_.p, iter_d_.p,
 	                           bad_d_.p);
+	a.wall_denom = wall_denom_d_.p;
 	launch_reduce<T>(a, f.Rc.p, f.Rd.p, p ? f.P1.p : f.P0.p, st_);
 	launch_halo<T>((int)halo_dst_.n, halo_dst_.p, halo_src_.p, NA_, p ? f.P1.p : f.P0.p, p ? f.P0.p : f.P1.p, st_);
 	launch_iter_advance(iter_d_.p, st_);
@@ -683,9 +776,10 @@ void Engine::export_state(void* host, size_t bytes) {
 	h.NA = NA_;
 	h.NR = NR_;
 	h.iters = total_iter_ + dev_iter_;
-	h.have_rms0 = have_rms0_ ? 1 : 0;
+	if (ncases_ != 1) throw Error(E3D_ERR_STATE, "state export covers single-case solvers");
+	h.have_rms0 = have_rms0_[0] ? 1 : 0;
 	h.carry = carry_;
-	for (int q = 0; q < 5; q++) h.rms0[q] = rms0_[q];
+	for (int q = 0; q < 5; q++) h.rms0[q] = rms0_[0][q];
 	std::memcpy(host, &h, sizeof(h));
 	char* p = static_cast<char*>(host) + sizeof(h);
 	const size_t pb = (opt_.precision == PREC_FP64 ? 8 : 4) * 5 * (size_t)NA_;
@@ -715,8 +809,9 @@ void Engine::import_state(const void* host, size_t bytes) {
 	cuda_ok(cudaStreamSynchronize(st_), "sync");
 	if (dev_iter_) collect_history(total_iter_, dev_iter_);
 	total_iter_ = (int)h.iters;
-	have_rms0_ = h.have_rms0 != 0;
-	for (int q = 0; q < 5; q++) rms0_[q] = h.rms0[q];
+	if (ncases_ != 1) throw Error(E3D_ERR_STATE, "state import covers single-case solvers");
+	have_rms0_[0] = h.have_rms0 != 0;
+	for (int q = 0; q < 5; q++) rms0_[0][q] = h.rms0[q];
 	started_ = true;
 }
 
@@ -732,28 +827,32 @@ void Engine::collect_history(int first_iter, int n) {
 	cuda_ok(cudaStreamSynchronize(st_), "sync");
 	dev_iter_ = 0;
 	for (int i = 0; i < n; i++) {
-		IterRecord r{};
-		r.iter = first_iter + i;
-		for (int b = 0; b < nb_; b++) {
-			const double* x = &h[((size_t)i * nb_ + b) * 10];
-			const double N = (double)(roff_[b + 1] - roff_[b]);
-			// Convergence::calculate*Rms (Convergence.cpp:27-48) then the block sum
-			// (BlockCommunicator.cpp:342-369)
-			for (int q = 0; q < 5; q++) r.rms[q] += (1. / N) * std::pow(x[q], 0.5);
-			// AerodynamicParameters::calculateGlobalCl/Cd (AerodynamicParameters.cpp:114-138)
-			const double cl_ = x[5], cd_ = x[6];
-			r.cl += cl_ * std::cos(aoa_rad_) - cd_ * std::sin(aoa_rad_);
-			r.cd += cl_ * std::sin(aoa_rad_) + cd_ * std::cos(aoa_rad_);
-			r.cmx += x[7];
-			r.cmy += x[8];
-			r.cmz += x[9];
+		for (int cs = 0; cs < ncases_; cs++) {
+			if (!case_active_[cs]) continue;
+			IterRecord r{};
+			r.iter = (int)hist_case_[cs].size();
+			const double aoa = case_aoa_[cs];
+			for (int b = case_boff_[cs]; b < case_boff_[cs + 1]; b++) {
+				const double* x = &h[((size_t)i * nb_ + b) * 10];
+				const double N = (double)(roff_[b + 1] - roff_[b]);
+				// Convergence::calculate*Rms (Convergence.cpp:27-48) then the block sum
+				// (BlockCommunicator.cpp:342-369)
+				for (int q = 0; q < 5; q++) r.rms[q] += (1. / N) * std::pow(x[q], 0.5);
+				// AerodynamicParameters::calculateGlobalCl/Cd (AerodynamicParameters.cpp:114-138)
+				const double cl_ = x[5], cd_ = x[6];
+				r.cl += cl_ * std::cos(aoa) - cd_ * std::sin(aoa);
+				r.cd += cl_ * std::sin(aoa) + cd_ * std::cos(aoa);
+				r.cmx += x[7];
+				r.cmy += x[8];
+				r.cmz += x[9];
+			}
+			if (!have_rms0_[cs]) {
+				for (int q = 0; q < 5; q++) rms0_[cs][q] = r.rms[q];
+				have_rms0_[cs] = 1;
+			}
+			for (int q = 0; q < 5; q++) r.conv[q] = std::log10(r.rms[q]) - std::log10(rms0_[cs][q]);
+			hist_case_[cs].push_back(r);
 		}
-		if (!have_rms0_) {
-			for (int q = 0; q < 5; q++) rms0_[q] = r.rms[q];
-			have_rms0_ = true;
-		}
-		for (int q = 0; q < 5; q++) r.conv[q] = std::log10(r.rms[q]) - std::log10(rms0_[q]);
-		hist_.push_back(r);
 	}
 	total_iter_ += n;
 	if (bad) throw Error(E3D_ERR_NONFINITE, "non-finite residual norm by iteration " + std::to_string(total_iter_ - 1));
@@ -763,6 +862,7 @@ int Engine::solve(int max_iter, double criterion, int check_every) {
 	if (check_every < 1) check_every = 1;
 	int done = 0;
 	while (true) {
+		const std::vector<IterRecord>& hist_ = hist_case_[0];
 		const size_t before = hist_.size();
 		iterate(std::min(check_every, std::max(1, max_iter - total_iter_)));
 		for (size_t i = before; i < hist_.size(); i++) {
@@ -1039,6 +1139,335 @@ std::vector<Engine::KernelTime> Engine::time_kernels(int n) {
 		}
 	}
 	return out;
+}
+
+}  // namespace e3d
+
+// ---------------------------------------------------------------- batches
+namespace e3d {
+
+namespace {
+// autotuning results per problem-size bucket (total cells rounded to a power
+// of two) and strategy; kept for the process and in $E3D_AUTOTUNE_CACHE if set
+struct TuneKey {
+	int bucket, scheme, grad, lim, order;
+	bool operator<(const TuneKey& o) const {
+		return std::tie(bucket, scheme, grad, lim, order) < std::tie(o.bucket, o.scheme, o.grad, o.lim, o.order);
+	}
+};
+std::map<TuneKey, std::pair<int, int>> g_tune;  // -> (tile_mult, blocks per SM)
+std::mutex g_tune_mu;
+
+void tune_cache_load() {
+	static bool loaded = false;
+	if (loaded) return;
+	loaded = true;
+	const char* path = std::getenv("E3D_AUTOTUNE_CACHE");
+	if (!path) return;
+	std::ifstream in(path);
+	TuneKey k;
+	int tm, bps;
+	while (in >> k.bucket >> k.scheme >> k.grad >> k.lim >> k.order >> tm >> bps) g_tune[k] = {tm, bps};
+}
+void tune_cache_store() {
+	const char* path = std::getenv("E3D_AUTOTUNE_CACHE");
+	if (!path) return;
+	std::ofstream out(path);
+	for (const auto& e : g_tune)
+		out << e.first.bucket << " " << e.first.scheme << " " << e.first.grad << " " << e.first.lim << " "
+		    << e.first.order << " " << e.second.first << " " << e.second.second << "\n";
+}
+}  // namespace
+
+// Work list: tiles of tile_mult * 128 consecutive real cells, never straddling
+// a block, for the blocks of active cases; block_work gives each block's range.
+void Engine::build_work() {
+	const int tile = tile_mult_ * kPersistThreads;
+	std::vector<int> work;
+	std::vector<int> bw(nb_ + 1, 0);
+	for (int b = 0; b < nb_; b++) {
+		if (case_active_[block_case_[b]])
+			for (int c = roff_[b]; c < roff_[b + 1]; c += tile) {
+				work.push_back(c);
+				work.push_back(std::min(c + tile, roff_[b + 1]));
+				work.push_back(b);
+				work.push_back(0);
+			}
+		bw[b + 1] = (int)work.size() / 4;
+	}
+	n_work_ = (int)work.size() / 4;
+	const size_t cap = 4 * ((size_t)NR_ / kPersistThreads + (size_t)nb_ + 1);
+	if (work_d_.n < cap) work_d_.alloc(cap);
+	if (wpart_d_.n < cap / 4 * 5) wpart_d_.alloc(cap / 4 * 5);
+	if (!work.empty())
+		cuda_ok(cudaMemcpyAsync(work_d_.p, work.data(), work.size() * sizeof(int), cudaMemcpyHostToDevice, st_), "work");
+	block_work_d_.upload(bw);
+	if (pgraph_) {
+		cudaGraphExecDestroy(pgraph_);
+		pgraph_ = nullptr;
+	}
+}
+
+// One cooperative launch of `iters` outer iterations over the work list,
+// through a captured CUDA graph when the capture succeeds.  Returns device ms.
+double Engine::run_persistent(int iters) {
+	return opt_.precision == PREC_FP32 ? run_persistent_t<float>(iters) : run_persistent_t<double>(iters);
+}
+
+template <class T>
+double Engine::run_persistent_t(int iters) {
+	if (n_work_ == 0 || iters <= 0) return 0.0;
+	if (!tet4_) throw Error(E3D_ERR_STATE, "the persistent batch kernel covers all-tetrahedron meshes");
+	if ((int)opt_.hist_capacity - dev_iter_ < iters) collect_history(total_iter_, dev_iter_);
+	if ((int)opt_.hist_capacity < iters) throw Error(E3D_ERR_LIMIT, "launch longer than the history capacity");
+	PersistArgs a{};
+	a.n_work = n_work_;
+	a.work = reinterpret_cast<const int4*>(work_d_.p);
+	a.block_work = block_work_d_.p;
+	a.nblocks = nb_;
+	a.stages = (int)alpha_.size();
+	for (int s = 0; s < a.stages; s++) {
+		a.alpha[s] = alpha_[s];
+		a.beta[s] = beta_[s];
+	}
+	a.carry = carry_;
+	a.iters = iters;
+	a.start_parity = cur_;
+	a.tile_mult = tile_mult_;
+	a.wpart = wpart_d_.p;
+	a.wall_off = wall_off_.p;
+	a.wall_face = wall_face_.p;
+	a.n_wall = (int)wall_face_.n;
+	a.wall_terms = wall_terms_.p;
+	a.wall_denom = wall_denom_d_.p;
+	a.denom = denom_;
+	a.face_lr = face_lr_.p;
+	a.S = S_.p;
+	a.fc = fc_.p;
+	a.hist = hist_d_.p;
+	a.stride = nb_ * 10;
+	a.d_iter = iter_d_.p;
+	a.hist_capacity = (int)opt_.hist_capacity;
+	a.d_bad = bad_d_.p;
+	a.n_halo = (int)halo_dst_.n;
+	a.halo_dst = halo_dst_.p;
+	a.halo_src = halo_src_.p;
+	Fused<T>& fb = fused<T>();
+	auto view = [&](bool flip) {
+		FusedView<T> v = fb.view(flip);
+		v.NR = NR_;
+		v.NG = NG_;
+		v.NA = NA_;
+		v.NS = NS_;
+		v.tet4 = tet4_;
+		v.slot_ptr = slot_ptr_.p;
+		v.slot_nbr = slot_nbr_.p;
+		v.slot_mate = slot_mate_.p;
+		v.gkind = gkind_.p;
+		v.grefl = grefl_.p;
+		v.W0 = W0_.p;
+		v.case_free = case_free_d_.p;
+		v.gcase = gcase_d_.p;
+		return v;
+	};
+	const FusedView<T> v0 = view(false), v1 = view(true);
+	const int grid = std::max(1, std::min(grid_, n_work_));
+	cudaEvent_t e0, e1;
+	cuda_ok(cudaEventCreate(&e0), "event");
+	cuda_ok(cudaEventCreate(&e1), "event");
+	cuda_ok(cudaEventRecord(e0, st_), "event");
+	bool launched = false;
+	if (opt_.use_graph) {
+		if (pgraph_ && (pgraph_iters_ != iters || pgraph_parity_ != cur_ || pgraph_grid_ != grid)) {
+			cudaGraphExecDestroy(pgraph_);
+			pgraph_ = nullptr;
+		}
+		if (!pgraph_) {
+			cudaGraph_t g;
+			if (cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+				const cudaError_t le =
+				    launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, order_ == 2, grid, st_);
+				const cudaError_t ce = cudaStreamEndCapture(st_, &g);
+				if (le == cudaSuccess && ce == cudaSuccess) {
+					if (cudaGraphInstantiate(&pgraph_, g, 0) != cudaSuccess) pgraph_ = nullptr;
+					cudaGraphDestroy(g);
+				} else if (ce == cudaSuccess) {
+					cudaGraphDestroy(g);
+				}
+				cudaGetLastError();
+			}
+			pgraph_iters_ = iters;
+			pgraph_parity_ = cur_;
+			pgraph_grid_ = grid;
+		}
+		if (pgraph_) {
+			cuda_ok(cudaGraphLaunch(pgraph_, st_), "graph launch");
+			launched = true;
+			tuning_.graph = true;
+		}
+	}
+	if (!launched)
+		cuda_ok(launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, order_ == 2, grid, st_),
+		        "cooperative launch");
+	cuda_ok(cudaEventRecord(e1, st_), "event");
+	cuda_ok(cudaEventSynchronize(e1), "event sync");
+	float ms = 0.f;
+	cuda_ok(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (alpha_.size() & 1) cur_ ^= (iters & 1);
+	dev_iter_ += iters;
+	started_ = true;
+	return (double)ms;
+}
+
+template double Engine::run_persistent_t<float>(int);
+template double Engine::run_persistent_t<double>(int);
+
+// Saves (save=true) or restores the state an iteration changes: both primitive
+// buffers, the FP64 W0 / carried state and the device iteration counter.
+void Engine::snapshot(bool save) {
+	const size_t ep = opt_.precision == PREC_FP32 ? sizeof(float) : sizeof(double);
+	const size_t np = (opt_.precision == PREC_FP32 ? f32_.P0.n : f64_.P0.n) * ep;
+	const size_t nw = W0_.n * sizeof(double);
+	if (snap_.n < 2 * np + nw + 16) snap_.alloc(2 * np + nw + 16);
+	void* p0 = opt_.precision == PREC_FP32 ? (void*)f32_.P0.p : (void*)f64_.P0.p;
+	void* p1 = opt_.precision == PREC_FP32 ? (void*)f32_.P1.p : (void*)f64_.P1.p;
+	unsigned char* b = snap_.p;
+	struct Part {
+		void* dev;
+		unsigned char* bak;
+		size_t n;
+	} parts[4] = {{p0, b, np}, {p1, b + np, np}, {W0_.p, b + 2 * np, nw}, {iter_d_.p, b + 2 * np + nw, sizeof(int)}};
+	for (const Part& q : parts)
+		if (q.n)
+			cuda_ok(cudaMemcpyAsync(save ? (void*)q.bak : q.dev, save ? q.dev : (void*)q.bak, q.n,
+			                        cudaMemcpyDeviceToDevice, st_),
+			        "snapshot");
+}
+
+// Picks the tile size (cells per work item) and the grid (resident blocks per
+// SM) by timing short launches on the live state, which is saved before and
+// restored after, so tuning never changes the solution; the choice is cached
+// per problem-size bucket (and in $E3D_AUTOTUNE_CACHE when set).
+void Engine::autotune(int iters) {
+	std::lock_guard<std::mutex> lk(g_tune_mu);
+	tune_cache_load();
+	int dev = 0, sms = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	const bool o2 = order_ == 2;
+	const int maxb = opt_.precision == PREC_FP32 ? persistent_blocks_per_sm<float>(grad_kind_, lim_kind_, scheme_, o2)
+	                                             : persistent_blocks_per_sm<double>(grad_kind_, lim_kind_, scheme_, o2);
+	if (maxb <= 0) throw Error(E3D_ERR_CUDA, "persistent kernel cannot be resident");
+	int bucket = 0;
+	while ((1LL << bucket) < (long long)NR_) bucket++;
+	const TuneKey key{bucket, scheme_, grad_kind_, lim_kind_, order_ + 4 * (int)opt_.precision};
+	auto it = g_tune.find(key);
+	if (it != g_tune.end()) {
+		tile_mult_ = it->second.first;
+		grid_ = std::min(maxb, it->second.second) * sms;
+		build_work();
+		tuning_.tile_cells = tile_mult_ * kPersistThreads;
+		tuning_.grid = grid_;
+		tuning_.from_cache = true;
+		return;
+	}
+	if ((int)opt_.hist_capacity - dev_iter_ < iters + 1) collect_history(total_iter_, dev_iter_);
+	const int dev_iter0 = dev_iter_, cur0 = cur_;
+	snapshot(true);
+	double best = 1e300;
+	int best_tm = 1, best_b = maxb;
+	for (int tm : {1, 2, 4}) {
+		tile_mult_ = tm;
+		build_work();
+		for (int b = maxb; b >= 1; b = b > 2 ? b - 2 : b - 1) {
+			grid_ = b * sms;
+			run_persistent(1);  // warm (and capture)
+			const double ms = run_persistent(iters) / iters;
+			if (ms < best) {
+				best = ms;
+				best_tm = tm;
+				best_b = b;
+			}
+			snapshot(false);
+			dev_iter_ = dev_iter0;
+			cur_ = cur0;
+		}
+	}
+	tile_mult_ = best_tm;
+	grid_ = best_b * sms;
+	build_work();
+	g_tune[key] = {best_tm, best_b};
+	tune_cache_store();
+	tuning_.tile_cells = best_tm * kPersistThreads;
+	tuning_.grid = grid_;
+	tuning_.ms_per_iter = best;
+	tuning_.from_cache = false;
+}
+
+double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch, std::vector<int>& iters_done) {
+	if (iters_per_launch < 1) iters_per_launch = 1;
+	if (!started_) halo();
+	collect_history(total_iter_, dev_iter_);
+	std::fill(case_active_.begin(), case_active_.end(), 1);
+	double ms_total = 0.0;
+	auto update_active = [&]() {
+		bool changed = false;
+		for (int c = 0; c < ncases_; c++) {
+			if (!case_active_[c]) continue;
+			const auto& h = hist_case_[c];
+			for (const IterRecord& r : h)
+				if (r.conv[0] <= criterion || (int)h.size() >= max_iter) {
+					case_active_[c] = 0;
+					changed = true;
+					break;
+				}
+		}
+		return changed;
+	};
+	if (grid_ == 0) {
+		cudaEvent_t e0, e1;
+		cuda_ok(cudaEventCreate(&e0), "event");
+		cuda_ok(cudaEventCreate(&e1), "event");
+		cuda_ok(cudaEventRecord(e0, st_), "event");
+		autotune(3);
+		cuda_ok(cudaEventRecord(e1, st_), "event");
+		cuda_ok(cudaEventSynchronize(e1), "event sync");
+		float ms = 0.f;
+		cudaEventElapsedTime(&ms, e0, e1);
+		ms_total += ms;
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		update_active();
+	}
+	build_work();
+	while (true) {
+		int room = max_iter;
+		bool any = false;
+		for (int c = 0; c < ncases_; c++)
+			if (case_active_[c]) {
+				any = true;
+				room = std::min(room, max_iter - (int)hist_case_[c].size());
+			}
+		if (!any || room <= 0) break;
+		ms_total += run_persistent(std::min(iters_per_launch, room));
+		collect_history(total_iter_, dev_iter_);
+		if (update_active()) build_work();
+	}
+	iters_done.assign(ncases_, 0);
+	for (int c = 0; c < ncases_; c++) {
+		const auto& h = hist_case_[c];
+		int n = (int)h.size();
+		for (int i = 0; i < (int)h.size(); i++)
+			if (h[i].conv[0] <= criterion) {
+				n = i + 1;
+				break;
+			}
+		iters_done[c] = n;
+	}
+	std::fill(case_active_.begin(), case_active_.end(), 1);
+	return ms_total;
 }
 
 }  // namespace e3d

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <memory>
 #include <string>
 #include <vector>
@@ -43,6 +44,10 @@ struct DevBuf {
 class Engine {
 public:
 	Engine(const HostCase& hc, const EngineOptions& opt);
+	// several cases advanced together in one device arena (a batch); they must
+	// share gamma, CFL, RK stages and the strategy choices, and may differ in
+	// mesh, Mach number, angle of attack and reference chord
+	Engine(const std::vector<const HostCase*>& cases, const EngineOptions& opt);
 	~Engine();
 	Engine(const Engine&) = delete;
 	Engine& operator=(const Engine&) = delete;
@@ -74,7 +79,22 @@ public:
 	// run until the reference stop test (max_iter or criterion) fires
 	int solve(int max_iter, double criterion, int check_every);
 
-	const std::vector<IterRecord>& history() const { return hist_; }
+	// --- batches: every active case advanced by the persistent cooperative
+	// kernel (FP32); a case stops (its tiles leave the work list) once its
+	// density drop reaches `criterion` or it has run max_iter iterations.
+	// iters_done[c] = iterations case c ran.  Returns the device time in ms.
+	double solve_batch(int max_iter, double criterion, int iters_per_launch, std::vector<int>& iters_done);
+	struct Tuning {
+		int tile_cells = 0, grid = 0;
+		double ms_per_iter = 0.0;
+		bool from_cache = false, graph = false;
+	};
+	const Tuning& tuning() const { return tuning_; }
+
+	const std::vector<IterRecord>& history() const { return hist_case_[0]; }
+	const std::vector<IterRecord>& history(int c) const { return hist_case_.at(c); }
+	int n_cases() const { return ncases_; }
+	long long n_real_case(int c) const;
 	void sync();  // waits for queued work; throws on a CUDA error or a non-finite norm
 
 	// --- state transfer (block-local cell order, FP64 on the host side)
@@ -110,7 +130,8 @@ private:
 		DevBuf<T> P0, P1, FS, Rc, Rd, dt, sgeo, sS, srv, lsw, vol;
 		FusedView<T> view(bool flip) const;
 	};
-	void build(const HostCase& hc);
+	void setup(const std::vector<const HostCase*>& cases);
+	void build_blocks(const std::vector<const HostBlock*>& blocks, const std::vector<Connexion>& conns);
 	void init_state();
 	void check(const char* what);
 	template <class T>
@@ -132,6 +153,12 @@ private:
 	std::vector<int> n_real_b_, n_all_b_;
 	Physics ph_{};
 	double denom_ = 1.0, aoa_rad_ = 0.0;
+	int ncases_ = 1;
+	std::vector<int> case_boff_;      // ncases+1 block offsets of each case
+	std::vector<int> block_case_;     // case of each block
+	std::vector<double> case_free_h_, case_denom_, case_aoa_;
+	DevBuf<double> case_free_d_, wall_denom_d_;
+	DevBuf<int> gcase_d_;
 	int carry_ = 0;
 	int grad_kind_ = GRAD_LEAST_SQUARES, lim_kind_ = LIM_VENKATAKRISHNAN, scheme_ = FLUX_ROE, order_ = 1;
 	std::vector<double> alpha_, beta_;
@@ -152,11 +179,37 @@ private:
 	int chunk_ = 0, max_chunks_ = 0;
 	int dev_iter_ = 0;  // iterations recorded on the device since the last collect
 	int total_iter_ = 0;
-	bool have_rms0_ = false;
-	double rms0_[5] = {0, 0, 0, 0, 0};
-	std::vector<IterRecord> hist_;
+	std::vector<char> have_rms0_;
+	std::vector<std::array<double, 5>> rms0_;
+	std::vector<std::vector<IterRecord>> hist_case_;
 	cudaGraphExec_t graph_[2] = {nullptr, nullptr};
+	// batch (persistent kernel) state
+	std::vector<char> case_active_;
+	DevBuf<int> work_d_, block_work_d_;
+	DevBuf<double> wpart_d_;
+	int n_work_ = 0, tile_mult_ = 1, grid_ = 0;
+	Tuning tuning_;
+	cudaGraphExec_t pgraph_ = nullptr;
+	int pgraph_iters_ = 0, pgraph_parity_ = -1, pgraph_grid_ = 0;
+	void build_work();
+	double run_persistent(int iters);
+	template <class T>
+	double run_persistent_t(int iters);
+	template <class T>
+	Fused<T>& fused();
+	void autotune(int iters);
+	void snapshot(bool save);
+	DevBuf<unsigned char> snap_;
 	size_t dev_bytes_ = 0;
 };
+
+template <>
+inline Engine::Fused<float>& Engine::fused<float>() {
+	return f32_;
+}
+template <>
+inline Engine::Fused<double>& Engine::fused<double>() {
+	return f64_;
+}
 
 }  // namespace e3d

@@ -10,4 +10,8 @@ template void launch_start<float>(const FusedView<float>&, const Physics&, int, 
 template void launch_flux_update<float>(const FusedView<float>&, const Physics&, int, bool, double, double, int, int,
                                         cudaStream_t);
 
+template int persistent_blocks_per_sm<float>(int, int, int, bool);
+template cudaError_t launch_persistent<float>(const FusedView<float>&, const FusedView<float>&, const Physics&,
+                                              const PersistArgs&, int, int, int, bool, int, cudaStream_t);
+
 }  // namespace e3d

@@ -64,5 +64,8 @@ template void launch_recon<double>(const FusedView<double>&, const Physics&, int
 template void launch_start<double>(const FusedView<double>&, const Physics&, int, cudaStream_t);
 template void launch_flux_update<double>(const FusedView<double>&, const Physics&, int, bool, double, double, int, int,
                                          cudaStream_t);
+template int persistent_blocks_per_sm<double>(int, int, int, bool);
+template cudaError_t launch_persistent<double>(const FusedView<double>&, const FusedView<double>&, const Physics&,
+                                               const PersistArgs&, int, int, int, bool, int, cudaStream_t);
 
 }  // namespace e3d

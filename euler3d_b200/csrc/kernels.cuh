@@ -9,6 +9,8 @@
 // in ascending face id, the reference's accumulation order, and no kernel uses
 // atomics: each cell (or ghost) is written by exactly one thread.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "physics.cuh"
 #include "views.hpp"
 
@@ -410,9 +412,7 @@ __device__ __forceinline__ void load_geo(const T* __restrict__ a, const SlotRang
 // face states of the cell and of its ghost cells.  FIRST additionally computes
 // W0 (unless carried) and the local time step from the stage-0 state.
 template <class T, int GRAD, int LIM, bool FIRST, int NSL>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_recon(FusedView<T> v, Physics ph, int carry_w0) {
-	const int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= v.NR) return;
+__device__ __forceinline__ void recon_cell(const FusedView<T>& v, const Physics& ph, int carry_w0, int c) {
 	const SlotRange<T, NSL> sr(v, c);
 	const Q5<T> q0 = ld5(v.Pin, v.NA, c);
 	int nb[MAXSL];
@@ -550,11 +550,15 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_recon(FusedView
 	}
 }
 
+template <class T, int GRAD, int LIM, bool FIRST, int NSL>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_recon(FusedView<T> v, Physics ph, int carry_w0) {
+	const int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c < v.NR) recon_cell<T, GRAD, LIM, FIRST, NSL>(v, ph, carry_w0, c);
+}
+
 // W0 and the local time step without a reconstruction pass (first order).
 template <class T, int NSL>
-__global__ void __launch_bounds__(128) k_start(FusedView<T> v, Physics ph, int carry_w0) {
-	const int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= v.NR) return;
+__device__ __forceinline__ void start_cell(const FusedView<T>& v, const Physics& ph, int carry_w0, int c) {
 	const SlotRange<T, NSL> sr(v, c);
 	const Q5<T> q0 = ld5(v.Pin, v.NA, c);
 	if (!carry_w0) {
@@ -575,6 +579,12 @@ __global__ void __launch_bounds__(128) k_start(FusedView<T> v, Physics ph, int c
 	v.dt[c] = T(ph.cfl) * v.vol[c] / srad;
 }
 
+template <class T, int NSL>
+__global__ void __launch_bounds__(128) k_start(FusedView<T> v, Physics ph, int carry_w0) {
+	const int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c < v.NR) start_cell<T, NSL>(v, ph, carry_w0, c);
+}
+
 // Pass 2 of a stage, one thread per real cell: convective and dissipative
 // fluxes of each face (computed identically from both sides), residual gather,
 // conservative update into Pout and the ghost states of the cell's boundary
@@ -586,9 +596,8 @@ __global__ void __launch_bounds__(128) k_start(FusedView<T> v, Physics ph, int c
 // Rd for finite fluxes, so the flux and the Rd store are skipped.  Rc is stored
 // only at the last stage, the one the norms (and callers) read.
 template <class T, int SCHEME, bool ORDER1, int NSL, bool DISS>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update(FusedView<T> v, Physics ph, T alpha, T beta, int last, int carry_w0) {
-	const int c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= v.NR) return;
+__device__ __forceinline__ void flux_update_cell(const FusedView<T>& v, const Physics& ph, T alpha, T beta, int last,
+                                                 int carry_w0, int c) {
 	const SlotRange<T, NSL> sr(v, c);
 	const T g = T(ph.gamma), gr = T(ph.gr), gm1 = T(ph.gm1);
 	int mate[MAXSL];
@@ -655,19 +664,30 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update(Fus
 	if (last && carry_w0)
 		for (int q = 0; q < 5; q++) v.W0[q * v.NR + c] = wn[q];
 	if (!ORDER1) load_int<T, NSL>(v.slot_nbr, sr, nb);
-	Q5<T> fr;
-	fr.r = T(ph.free[0]);
-	fr.u = T(ph.free[1]);
-	fr.v = T(ph.free[2]);
-	fr.w = T(ph.free[3]);
-	fr.p = T(ph.free[4]);
 #pragma unroll
 	E3D_SLOTS(k, sr) {
 		if (nb[k] >= v.NR) {
-			const int kind = v.gkind[nb[k] - v.NR];
-			if (kind != GK_NONE) st5(v.Pout, v.NA, nb[k], ghost_state(kind, qnew, fr, geo[k][0], geo[k][1], geo[k][2], g));
+			const int gi = nb[k] - v.NR;
+			const int kind = v.gkind[gi];
+			if (kind != GK_NONE) {
+				// freestream of the ghost's case (batched cases differ in Mach and alpha)
+				const double* f = v.case_free ? v.case_free + 5 * v.gcase[gi] : ph.free;
+				Q5<T> fr;
+				fr.r = T(f[0]);
+				fr.u = T(f[1]);
+				fr.v = T(f[2]);
+				fr.w = T(f[3]);
+				fr.p = T(f[4]);
+				st5(v.Pout, v.NA, nb[k], ghost_state(kind, qnew, fr, geo[k][0], geo[k][1], geo[k][2], g));
+			}
 		}
 	}
+}
+
+template <class T, int SCHEME, bool ORDER1, int NSL, bool DISS>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update(FusedView<T> v, Physics ph, T alpha, T beta, int last, int carry_w0) {
+	const int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c < v.NR) flux_update_cell<T, SCHEME, ORDER1, NSL, DISS>(v, ph, alpha, beta, last, carry_w0, c);
 }
 
 // ===================================================================== reductions
@@ -719,13 +739,14 @@ __global__ void k_norm_final(const double* __restrict__ partial, int nblocks, in
 template <class T>
 __global__ void k_wall_terms(const T* __restrict__ P, int NA, int nwall, const int* __restrict__ wall_face,
                              const int* __restrict__ face_lr, const double* __restrict__ S,
-                             const double* __restrict__ fc, double denom, double* __restrict__ terms) {
+                             const double* __restrict__ fc, double denom, const double* __restrict__ wall_denom,
+                             double* __restrict__ terms) {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= nwall) return;
 	const int f = wall_face[i];
 	const double p0 = (double)P[4 * (size_t)NA + face_lr[2 * f]], p1 = (double)P[4 * (size_t)NA + face_lr[2 * f + 1]];
 	const double pbc = 0.5 * (p0 + p1);
-	const double cp = (pbc - 1.) / denom;
+	const double cp = (pbc - 1.) / (wall_denom ? wall_denom[i] : denom);
 	const double fx = cp * S[3 * f], fy = cp * S[3 * f + 1], fz = cp * S[3 * f + 2];
 	const double x = fc[3 * f], y = fc[3 * f + 1], z = fc[3 * f + 2];
 	terms[i] = fy;
@@ -759,6 +780,135 @@ __global__ void __launch_bounds__(128) k_wall_sums(const double* __restrict__ te
 }
 
 __global__ void k_iter_advance(int* d_iter) { *d_iter += 1; }
+
+
+// ===================================================================== persistent
+// Batched cases: one cooperative launch runs `iters` outer iterations over the
+// work list.  Phases are separated by grid-wide barriers: per stage the
+// reconstruction pass and the flux/update pass (the same per-cell functions as
+// the one-kernel-per-pass path), then per iteration the norm partials, wall
+// terms and halo, then the per-block sums into the history.  Tiles of
+// converged cases are simply absent from the work list.
+template <class T, int GRAD, int LIM, int SCHEME, bool ORDER2, int TPB>
+__global__ void __launch_bounds__(TPB, 512 / TPB) k_persistent(FusedView<T> v0, FusedView<T> v1, Physics ph,
+                                                               PersistArgs a) {
+	namespace cg = cooperative_groups;
+	cg::grid_group grid = cg::this_grid();
+	__shared__ double red[5][TPB];
+	__shared__ double wbuf[5][WALL_CHUNK / 4];
+	const int base = *a.d_iter;
+	int parity = a.start_parity;  // which primitive buffer holds the current state
+	for (int it = 0; it < a.iters; it++) {
+		for (int s = 0; s < a.stages; s++) {
+			const FusedView<T>& v = parity ? v1 : v0;
+			if (ORDER2 || s == 0) {
+				for (int w = blockIdx.x; w < a.n_work; w += gridDim.x) {
+					const int4 t = a.work[w];
+					for (int c = t.x + threadIdx.x; c < t.y; c += TPB) {
+						if (ORDER2) {
+							if (s == 0) recon_cell<T, GRAD, LIM, true, 4>(v, ph, a.carry, c);
+							else recon_cell<T, GRAD, LIM, false, 4>(v, ph, a.carry, c);
+						} else {
+							start_cell<T, 4>(v, ph, a.carry, c);
+						}
+					}
+				}
+				grid.sync();
+			}
+			const T al = T(a.alpha[s]), be = T(a.beta[s]);
+			const int last = s == a.stages - 1;
+			for (int w = blockIdx.x; w < a.n_work; w += gridDim.x) {
+				const int4 t = a.work[w];
+				for (int c = t.x + threadIdx.x; c < t.y; c += TPB) {
+					if (a.beta[s] != 0.0) flux_update_cell<T, SCHEME, !ORDER2, 4, true>(v, ph, al, be, last, a.carry, c);
+					else flux_update_cell<T, SCHEME, !ORDER2, 4, false>(v, ph, al, be, last, a.carry, c);
+				}
+			}
+			grid.sync();
+			parity ^= 1;
+		}
+		const FusedView<T>& vf = parity ? v1 : v0;  // Pin of the next stage = current state
+		// per-tile residual sums (fixed tree order)
+		for (int w = blockIdx.x; w < a.n_work; w += gridDim.x) {
+			const int4 t = a.work[w];
+			double acc[5] = {0., 0., 0., 0., 0.};
+			for (int c = t.x + threadIdx.x; c < t.y; c += TPB)
+				for (int q = 0; q < 5; q++) {
+					const double r = (double)vf.Rc[q * vf.NR + c] - (double)vf.Rd[q * vf.NR + c];
+					acc[q] += r * r;
+				}
+			for (int q = 0; q < 5; q++) red[q][threadIdx.x] = acc[q];
+			__syncthreads();
+			for (int h = TPB / 2; h > 0; h >>= 1) {
+				if (threadIdx.x < h)
+					for (int q = 0; q < 5; q++) red[q][threadIdx.x] += red[q][threadIdx.x + h];
+				__syncthreads();
+			}
+			if (threadIdx.x < 5) a.wpart[(size_t)w * 5 + threadIdx.x] = red[threadIdx.x][0];
+			__syncthreads();
+		}
+		// wall terms of every wall face (frozen cases included: cheap, ignored by the host)
+		for (int i = blockIdx.x * TPB + threadIdx.x; i < a.n_wall; i += gridDim.x * TPB) {
+			const int f = a.wall_face[i];
+			const double p0 = (double)vf.Pin[4 * (size_t)vf.NA + a.face_lr[2 * f]];
+			const double p1 = (double)vf.Pin[4 * (size_t)vf.NA + a.face_lr[2 * f + 1]];
+			const double cp = (0.5 * (p0 + p1) - 1.) / (a.wall_denom ? a.wall_denom[i] : a.denom);
+			const double fx = cp * a.S[3 * f], fy = cp * a.S[3 * f + 1], fz = cp * a.S[3 * f + 2];
+			const double x = a.fc[3 * f], y = a.fc[3 * f + 1], z = a.fc[3 * f + 2];
+			a.wall_terms[i] = fy;
+			a.wall_terms[(size_t)a.n_wall + i] = fx;
+			a.wall_terms[2 * (size_t)a.n_wall + i] = y * fz - z * fy;
+			a.wall_terms[3 * (size_t)a.n_wall + i] = z * fx - x * fz;
+			a.wall_terms[4 * (size_t)a.n_wall + i] = x * fy - y * fx;
+		}
+		// inter-block halo into both primitive buffers
+		for (int i = blockIdx.x * TPB + threadIdx.x; i < a.n_halo; i += gridDim.x * TPB) {
+			const Q5<T> q = ld5(vf.Pin, vf.NA, a.halo_src[i]);
+			st5(const_cast<T*>(vf.Pin), vf.NA, a.halo_dst[i], q);
+			st5(vf.Pout, vf.NA, a.halo_dst[i], q);
+		}
+		grid.sync();
+		// per-block sums into the history: tiles in a fixed tree order, wall
+		// faces sequentially in the reference's order
+		const int slot = min(base + it, a.hist_capacity - 1);
+		for (int b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
+			const int w0 = a.block_work[b], w1 = a.block_work[b + 1];
+			double acc[5] = {0., 0., 0., 0., 0.};
+			for (int w = w0 + threadIdx.x; w < w1; w += TPB)
+				for (int q = 0; q < 5; q++) acc[q] += a.wpart[(size_t)w * 5 + q];
+			for (int q = 0; q < 5; q++) red[q][threadIdx.x] = acc[q];
+			__syncthreads();
+			for (int h = TPB / 2; h > 0; h >>= 1) {
+				if (threadIdx.x < h)
+					for (int q = 0; q < 5; q++) red[q][threadIdx.x] += red[q][threadIdx.x + h];
+				__syncthreads();
+			}
+			double* out = a.hist + (size_t)slot * a.stride + b * 10;
+			if (threadIdx.x < 5) {
+				out[threadIdx.x] = red[threadIdx.x][0];
+				if (!isfinite(red[threadIdx.x][0]) && w1 > w0) *a.d_bad = 1;
+			}
+			const int beg = a.wall_off[b], end = a.wall_off[b + 1];
+			double fs = 0.;
+			constexpr int CH = WALL_CHUNK / 4;
+			for (int base_i = beg; base_i < end; base_i += CH) {
+				const int n = min(CH, end - base_i);
+				__syncthreads();
+				for (int j = threadIdx.x; j < 5 * n; j += TPB) {
+					const int q = j / n, i = j - q * n;
+					wbuf[q][i] = a.wall_terms[(size_t)q * a.n_wall + base_i + i];
+				}
+				__syncthreads();
+				if (threadIdx.x < 5)
+					for (int i = 0; i < n; i++) fs += wbuf[threadIdx.x][i];
+			}
+			if (threadIdx.x < 5) out[5 + threadIdx.x] = fs;
+			__syncthreads();
+		}
+		grid.sync();
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) *a.d_iter = base + a.iters;
+}
 
 }  // namespace
 }  // namespace e3d

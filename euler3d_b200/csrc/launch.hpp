@@ -40,6 +40,7 @@ struct ReduceArgs {
 	const double* S;
 	const double* fc;
 	double denom;          // 0.5*gamma*M*M*cmac
+	const double* wall_denom;  // per wall face (cases of a batch differ in Mach), or null
 	double* hist;
 	int stride;
 	const int* d_iter;
@@ -54,6 +55,14 @@ template <class T>
 void launch_recon(const FusedView<T>&, const Physics&, int grad, int lim, bool first, int carry, cudaStream_t);
 template <class T>
 void launch_start(const FusedView<T>&, const Physics&, int carry, cudaStream_t);
+
+// persistent batch kernel: threads per block, resident blocks per SM, launch
+constexpr int kPersistThreads = 128;
+template <class T>
+int persistent_blocks_per_sm(int grad, int lim, int scheme, bool order2);
+template <class T>
+cudaError_t launch_persistent(const FusedView<T>& v0, const FusedView<T>& v1, const Physics& ph, const PersistArgs& a,
+                              int grad, int lim, int scheme, bool order2, int grid, cudaStream_t st);
 
 template <class T>
 void launch_flux_update(const FusedView<T>&, const Physics&, int scheme, bool order1, double alpha, double beta,

@@ -19,7 +19,7 @@ void launch_reduce(const ReduceArgs& a, const T* Rc, const T* Rd, const T* P, cu
 	                                                         a.d_iter, a.d_bad);
 	if (a.n_wall > 0)
 		k_wall_terms<T><<<(a.n_wall + 127) / 128, 128, 0, st>>>(P, a.NA, a.n_wall, a.wall_face, a.face_lr, a.S, a.fc,
-		                                                     a.denom, a.wall_terms);
+		                                                     a.denom, a.wall_denom, a.wall_terms);
 	k_wall_sums<<<a.nblocks, 128, 0, st>>>(a.wall_terms, a.n_wall, a.wall_off, a.hist, a.stride, a.d_iter);
 }
 
@@ -82,6 +82,51 @@ void launch_flux_update(const FusedView<T>& v, const Physics& ph, int scheme, bo
 		else E3D_FLUX(FLUX_ROE, false);
 	}
 #undef E3D_FLUX
+}
+
+// ---- persistent batch kernel (cooperative launch)
+constexpr int PERSIST_TPB = 128;
+
+template <class T, int GRAD, int LIM, int SCHEME, bool ORDER2>
+void* persistent_fn() {
+	return reinterpret_cast<void*>(&k_persistent<T, GRAD, LIM, SCHEME, ORDER2, PERSIST_TPB>);
+}
+
+template <class T>
+void* persistent_select(int grad, int lim, int scheme, bool order2) {
+#define E3D_P(G, L, S)                                                                      \
+	if (grad == G && lim == L && scheme == S)                                               \
+		return order2 ? persistent_fn<T, G, L, S, true>() : persistent_fn<T, G, L, S, false>();
+	E3D_P(GRAD_GREEN_GAUSS, LIM_BARTH_JESPERSEN, FLUX_ROE)
+	E3D_P(GRAD_GREEN_GAUSS, LIM_BARTH_JESPERSEN, FLUX_AUSM)
+	E3D_P(GRAD_GREEN_GAUSS, LIM_VENKATAKRISHNAN, FLUX_ROE)
+	E3D_P(GRAD_GREEN_GAUSS, LIM_VENKATAKRISHNAN, FLUX_AUSM)
+	E3D_P(GRAD_LEAST_SQUARES, LIM_BARTH_JESPERSEN, FLUX_ROE)
+	E3D_P(GRAD_LEAST_SQUARES, LIM_BARTH_JESPERSEN, FLUX_AUSM)
+	E3D_P(GRAD_LEAST_SQUARES, LIM_VENKATAKRISHNAN, FLUX_ROE)
+	E3D_P(GRAD_LEAST_SQUARES, LIM_VENKATAKRISHNAN, FLUX_AUSM)
+#undef E3D_P
+	return nullptr;
+}
+
+template <class T>
+int persistent_blocks_per_sm(int grad, int lim, int scheme, bool order2) {
+	int n = 0;
+	void* fn = persistent_select<T>(grad, lim, scheme, order2);
+	if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, PERSIST_TPB, 0) != cudaSuccess) return 0;
+	return n;
+}
+
+template <class T>
+cudaError_t launch_persistent(const FusedView<T>& v0, const FusedView<T>& v1, const Physics& ph, const PersistArgs& a,
+                              int grad, int lim, int scheme, bool order2, int grid, cudaStream_t st) {
+	void* fn = persistent_select<T>(grad, lim, scheme, order2);
+	if (!fn) return cudaErrorInvalidValue;
+	FusedView<T> x0 = v0, x1 = v1;
+	Physics p = ph;
+	PersistArgs q = a;
+	void* args[] = {&x0, &x1, &p, &q};
+	return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(PERSIST_TPB), args, 0, st);
 }
 
 }  // namespace e3d

@@ -76,6 +76,43 @@ struct FusedView {
 	T* Rd;                  // 5*NR
 	double* W0;             // 5*NR
 	T* dt;                  // NR
+	const double* case_free;  // 5 per case, or null: every ghost uses Physics::free
+	const int* gcase;         // NG case index of each ghost (with case_free)
+};
+
+// One launch of the persistent batch kernel: several outer iterations over the
+// work list (tiles of real cells of the active cases).
+struct PersistArgs {
+	int n_work;            // work items (tiles)
+	const int4* work;      // x: first cell, y: end cell, z: block, w: unused
+	const int* block_work; // nblocks+1: work items of block b are [block_work[b], block_work[b+1])
+	int nblocks;
+	int stages;
+	double alpha[5], beta[5];
+	int carry;
+	int iters;             // outer iterations in this launch
+	int start_parity;      // 0: state in P0 (view v0 reads it), 1: state in P1
+	int tile_mult;         // a work item covers tile_mult * blockDim cells
+	// reductions
+	double* wpart;         // n_work*5 per-tile sums of (Rc-Rd)^2
+	const int* wall_off;
+	const int* wall_face;
+	int n_wall;
+	double* wall_terms;
+	const double* wall_denom;
+	double denom;
+	const int* face_lr;
+	const double* S;
+	const double* fc;
+	double* hist;          // [iteration][block][10]
+	int stride;
+	int* d_iter;           // iteration counter (advanced by `iters` at the end)
+	int hist_capacity;
+	int* d_bad;
+	// halo
+	int n_halo;
+	const int* halo_dst;
+	const int* halo_src;
 };
 
 }  // namespace e3d

@@ -149,6 +149,27 @@ int e3d_history(const e3d_solver* s, int first, int count, e3d_iter_record* out)
 int e3d_state_get(e3d_solver* s, int block, const char* name, double* dst, int64_t count);
 int e3d_state_set(e3d_solver* s, int block, const char* name, const double* src, int64_t count);
 
+/* ---- batches of cases (Mach / alpha sweeps on meshes of uneven size) ----------
+ * No counterpart in the reference (one case per run).  e3d_batch_create puts
+ * every block of every case in one device arena; the cases must share gamma,
+ * CFL, RK stages and the strategy choices and may differ in mesh, Mach, alpha
+ * and chord.  e3d_batch_solve advances all cases together with the persistent
+ * cooperative kernel (FP32 variant, tetrahedral meshes): one graph-captured
+ * launch runs `iters_per_launch` outer iterations over a work list of tiles;
+ * a case leaves the work list once its density drop reaches `criterion` or it
+ * has run max_iter iterations.  The first call autotunes the tile size and
+ * the grid (cached per problem-size bucket, and in $E3D_AUTOTUNE_CACHE if set).
+ * iters_done[c] = iterations case c needed (n_cases entries);
+ * *device_ms = device time of the whole solve.  e3d_iterate also works on a
+ * batch (every case advances; no per-case stop). */
+int e3d_batch_create(const e3d_case* const* cases, int n_cases, const e3d_options* opt, e3d_solver** out);
+int e3d_batch_solve(e3d_solver* s, int max_iter, double criterion, int iters_per_launch, int* iters_done,
+                    double* device_ms);
+int e3d_case_count(const e3d_solver* s, int* n);
+int e3d_case_history_length(const e3d_solver* s, int case_index, int* n);
+int e3d_case_history(const e3d_solver* s, int case_index, int first, int count, e3d_iter_record* out);
+int e3d_batch_tuning(const e3d_solver* s, int* tile_cells, int* grid, double* ms_per_iter, int* from_cache);
+
 /* Checkpoint / restart of the whole solver state (the reference's restart
  * writer is an empty stub, PostProcessing/src/OutputTecplot.cpp:475-494):
  * current primitives of every cell in the solver precision, the FP64
