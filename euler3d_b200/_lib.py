@@ -22,6 +22,7 @@ GRAD = {"greengauss": 0, "leastsquares": 1}
 LIM = {"barthjespersen": 0, "venkatakrishnan": 1}
 FLUX = {"roe": 0, "ausm": 1}
 FP64, FP32 = 0, 1
+SURROGATE_PARAMS, SURROGATE_NORM = 36232, 24
 
 
 class E3DError(RuntimeError):
@@ -102,6 +103,21 @@ SIGNATURES = {
     "e3d_case_history": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "e3d_batch_tuning": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
                           C.POINTER(C.c_int)], C.c_int),
+    "e3d_solver_set_precision": ([C.c_void_p, C.c_int], C.c_int),
+    "e3d_cell_features": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "e3d_surrogate_create": ([C.c_int, C.c_uint64, C.c_double, C.POINTER(C.c_void_p)], C.c_int),
+    "e3d_surrogate_free": ([C.c_void_p], C.c_int),
+    "e3d_surrogate_add_solution": ([C.c_void_p, C.c_void_p], C.c_int),
+    "e3d_surrogate_add_samples": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "e3d_surrogate_sample_count": ([C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
+    "e3d_surrogate_clear": ([C.c_void_p], C.c_int),
+    "e3d_surrogate_train": ([C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.POINTER(C.c_double)], C.c_int),
+    "e3d_surrogate_gradient": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_double)],
+                               C.c_int),
+    "e3d_surrogate_predict": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p], C.c_int),
+    "e3d_surrogate_get_params": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "e3d_surrogate_set_params": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "e3d_warm_start": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "e3d_residual_norms_noalloc": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                     C.c_void_p], C.c_int),
 }

@@ -250,6 +250,96 @@ class Batch(Solver):
         return {"tile_cells": t.value, "grid": g.value, "ms_per_iter": ms.value, "from_cache": bool(fc.value)}
 
 
+def set_precision(solver: Solver, precision: str) -> None:
+    """Switch an FP32 solver (or batch) to FP64 in place."""
+    L.check(L.lib().e3d_solver_set_precision(solver._h, L.FP64 if precision == "fp64" else L.FP32))
+    solver.precision = precision
+
+
+def cell_features(solver: Solver) -> np.ndarray:
+    """Surrogate inputs of every real cell, [n_real_total, 8] float32 (x, y, z, wall distance, Mach, alpha, 0, 0)."""
+    n = sum(i.n_real for i in solver._info)
+    out = np.empty((n, 8), dtype=np.float32)
+    L.check(L.lib().e3d_cell_features(solver._h, L.ptr(out), out.size))
+    return out
+
+
+class Surrogate:
+    """The per-cell warm-start MLP (6 -> 128 -> 128 -> 128 -> 5, GELU, BF16 weights, FP32 accumulation)."""
+
+    N_PARAMS, N_NORM = L.SURROGATE_PARAMS, L.SURROGATE_NORM
+
+    def __init__(self, seed: int = 0, gamma: float = 1.4, device: int = -1):
+        h = C.c_void_p()
+        L.check(L.lib().e3d_surrogate_create(device, seed, gamma, C.byref(h)))
+        self._h = h
+
+    def add_solution(self, solver: Solver) -> None:
+        L.check(L.lib().e3d_surrogate_add_solution(self._h, solver._h))
+
+    def add_samples(self, features: np.ndarray, states: np.ndarray) -> None:
+        f = np.ascontiguousarray(features[:, :6], dtype=np.float32)
+        w = np.ascontiguousarray(states[:, :5], dtype=np.float32)
+        L.check(L.lib().e3d_surrogate_add_samples(self._h, L.ptr(f), L.ptr(w), f.shape[0]))
+
+    @property
+    def n_samples(self) -> int:
+        n = C.c_int64()
+        L.check(L.lib().e3d_surrogate_sample_count(self._h, C.byref(n)))
+        return n.value
+
+    def clear(self) -> None:
+        L.check(L.lib().e3d_surrogate_clear(self._h))
+
+    def train(self, steps: int, batch: int = 16384, lr: float = 2e-3) -> tuple[float, np.ndarray]:
+        hist = np.zeros(max(1, steps), dtype=np.float32)
+        loss = C.c_double()
+        L.check(L.lib().e3d_surrogate_train(self._h, steps, batch, lr, L.ptr(hist), C.byref(loss)))
+        return loss.value, hist[:steps]
+
+    def gradient(self, features: np.ndarray, states: np.ndarray) -> tuple[float, np.ndarray]:
+        f = np.ascontiguousarray(features[:, :6], dtype=np.float32)
+        w = np.ascontiguousarray(states[:, :5], dtype=np.float32)
+        g = np.zeros(self.N_PARAMS, dtype=np.float32)
+        loss = C.c_double()
+        L.check(L.lib().e3d_surrogate_gradient(self._h, L.ptr(f), L.ptr(w), f.shape[0], L.ptr(g), C.byref(loss)))
+        return loss.value, g
+
+    def predict(self, features: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(features[:, :6], dtype=np.float32)
+        out = np.zeros((f.shape[0], 5), dtype=np.float32)
+        L.check(L.lib().e3d_surrogate_predict(self._h, L.ptr(f), f.shape[0], L.ptr(out)))
+        return out
+
+    def get_params(self) -> tuple[np.ndarray, np.ndarray]:
+        p = np.zeros(self.N_PARAMS, dtype=np.float32)
+        n = np.zeros(self.N_NORM, dtype=np.float32)
+        L.check(L.lib().e3d_surrogate_get_params(self._h, L.ptr(p), L.ptr(n)))
+        return p, n
+
+    def set_params(self, params: np.ndarray | None = None, norm: np.ndarray | None = None) -> None:
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        n = None if norm is None else np.ascontiguousarray(norm, dtype=np.float32)
+        L.check(L.lib().e3d_surrogate_set_params(self._h, None if p is None else L.ptr(p),
+                                                 None if n is None else L.ptr(n)))
+
+    def warm_start(self, solver: Solver) -> int:
+        n = C.c_int()
+        L.check(L.lib().e3d_warm_start(solver._h, self._h, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().e3d_surrogate_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # --------------------------------------------------------------------------------
 # Strategy classes with the reference's names.  A ``Block`` is one block of a
 # device-resident solver (the reference's Block*); methods launch one kernel.

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "engine.hpp"
+#include "surrogate.hpp"
 #include "mesh.hpp"
 
 struct e3d_case {
@@ -13,6 +14,9 @@ struct e3d_case {
 };
 struct e3d_solver {
 	std::unique_ptr<e3d::Engine> eng;
+};
+struct e3d_surrogate {
+	std::unique_ptr<e3d::Surrogate> net;
 };
 
 namespace {
@@ -294,6 +298,126 @@ int e3d_batch_tuning(const e3d_solver* s, int* tile_cells, int* grid, double* ms
 	if (ms_per_iter) *ms_per_iter = t.ms_per_iter;
 	if (from_cache) *from_cache = t.from_cache ? 1 : 0;
 	return E3D_OK;
+}
+
+int e3d_solver_set_precision(e3d_solver* s, int precision) {
+	return guard([&] {
+		if (precision == E3D_FP64) eng(s).widen_to_fp64();
+		else if (eng(s).precision() != e3d::PREC_FP32)
+			throw e3d::Error(E3D_ERR_ARG, "a solver switches from FP32 to FP64 only");
+	});
+}
+
+int e3d_cell_features(e3d_solver* s, float* out, int64_t n_floats) {
+	return guard([&] {
+		e3d::Engine& e = eng(s);
+		const long long nr = e.n_real_total();
+		if (!out || n_floats < 8 * nr) throw e3d::Error(E3D_ERR_ARG, "feature buffer too small");
+		e3d::DevBuf<float> d;
+		d.alloc((size_t)nr * 8);
+		e.cell_features(d.p);
+		e3d::cuda_ok(cudaMemcpyAsync(out, d.p, (size_t)nr * 8 * sizeof(float), cudaMemcpyDeviceToHost, e.stream()),
+		             "features");
+		e3d::cuda_ok(cudaStreamSynchronize(e.stream()), "sync");
+	});
+}
+
+static e3d::Surrogate& net(e3d_surrogate* m) {
+	if (!m || !m->net) throw e3d::Error(E3D_ERR_ARG, "null surrogate");
+	return *m->net;
+}
+
+int e3d_surrogate_create(int device, uint64_t seed, double gamma, e3d_surrogate** out) {
+	if (!out) return fail(E3D_ERR_ARG, "null argument");
+	*out = nullptr;
+	return guard([&] {
+		static_assert(e3d::SurrogateShape::N_PARAM == E3D_SURROGATE_PARAMS, "parameter count");
+		static_assert(e3d::SurrogateShape::N_NORM == E3D_SURROGATE_NORM, "normalisation count");
+		if (!(gamma > 1.0)) throw e3d::Error(E3D_ERR_ARG, "gamma must exceed 1");
+		auto* m = new e3d_surrogate;
+		try {
+			m->net.reset(new e3d::Surrogate(device, seed, gamma));
+		} catch (...) {
+			delete m;
+			throw;
+		}
+		*out = m;
+	});
+}
+
+int e3d_surrogate_free(e3d_surrogate* m) {
+	return guard([&] { delete m; });
+}
+
+int e3d_surrogate_add_solution(e3d_surrogate* m, e3d_solver* s) {
+	return guard([&] { net(m).add_solution(eng(s)); });
+}
+
+int e3d_surrogate_add_samples(e3d_surrogate* m, const float* features6, const float* states5, int64_t n) {
+	return guard([&] {
+		if (n < 0 || (n > 0 && (!features6 || !states5))) throw e3d::Error(E3D_ERR_ARG, "bad sample arrays");
+		net(m).add_samples_host(features6, states5, n);
+	});
+}
+
+int e3d_surrogate_sample_count(const e3d_surrogate* m, int64_t* n) {
+	if (!m || !m->net || !n) return fail(E3D_ERR_ARG, "null argument");
+	*n = m->net->n_samples();
+	return E3D_OK;
+}
+
+int e3d_surrogate_clear(e3d_surrogate* m) {
+	return guard([&] { net(m).clear_samples(); });
+}
+
+int e3d_surrogate_train(e3d_surrogate* m, int steps, int batch, double lr, float* loss_per_step, double* final_loss) {
+	return guard([&] {
+		if (steps < 0 || !(lr > 0.0)) throw e3d::Error(E3D_ERR_ARG, "steps must be >= 0 and lr > 0");
+		std::vector<float> h;
+		const double l = net(m).train(steps, batch, lr, loss_per_step ? &h : nullptr);
+		if (loss_per_step) std::copy(h.begin(), h.end(), loss_per_step);
+		if (final_loss) *final_loss = l;
+	});
+}
+
+int e3d_surrogate_gradient(e3d_surrogate* m, const float* features6, const float* states5, int n, float* grad,
+                           double* loss) {
+	return guard([&] {
+		if (!features6 || !states5 || !grad) throw e3d::Error(E3D_ERR_ARG, "null argument");
+		std::vector<float> g;
+		const double l = net(m).gradient(features6, states5, n, g);
+		std::copy(g.begin(), g.end(), grad);
+		if (loss) *loss = l;
+	});
+}
+
+int e3d_surrogate_predict(e3d_surrogate* m, const float* features6, int64_t n, float* states5) {
+	return guard([&] {
+		if (n < 0 || (n > 0 && (!features6 || !states5))) throw e3d::Error(E3D_ERR_ARG, "bad arrays");
+		net(m).predict_host(features6, n, states5);
+	});
+}
+
+int e3d_surrogate_get_params(const e3d_surrogate* m, float* params, float* norm) {
+	return guard([&] {
+		if (!m || !m->net) throw e3d::Error(E3D_ERR_ARG, "null surrogate");
+		if (params) m->net->get_params(params);
+		if (norm) m->net->get_normalisation(norm);
+	});
+}
+
+int e3d_surrogate_set_params(e3d_surrogate* m, const float* params, const float* norm) {
+	return guard([&] {
+		if (params) net(m).set_params(params);
+		if (norm) net(m).set_normalisation(norm);
+	});
+}
+
+int e3d_warm_start(e3d_solver* s, e3d_surrogate* m, int* n_fallback) {
+	return guard([&] {
+		const int n = net(m).warm_start(eng(s));
+		if (n_fallback) *n_fallback = n;
+	});
 }
 
 int e3d_solver_free(e3d_solver* s) {

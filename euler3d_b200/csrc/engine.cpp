@@ -1,6 +1,7 @@
 // Device-resident solver: global numbering, uploads, stage sequencing and the
 // captured outer iteration.
 #include "engine.hpp"
+#include "warm.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -12,12 +13,6 @@
 #include <tuple>
 
 namespace e3d {
-
-namespace {
-void cuda_ok(cudaError_t e, const char* what) {
-	if (e != cudaSuccess) throw Error(E3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-}
-}  // namespace
 
 template <class T>
 void DevBuf<T>::alloc(size_t count) {
@@ -41,6 +36,7 @@ template struct DevBuf<signed char>;
 template struct DevBuf<double>;
 template struct DevBuf<float>;
 template struct DevBuf<unsigned char>;
+template struct DevBuf<unsigned short>;
 
 template <class T>
 FusedView<T> Engine::Fused<T>::view(bool flip) const {
@@ -127,6 +123,8 @@ Engine::Engine(const std::vector<const HostCase*>& cases, const EngineOptions& o
 		case_free_h_.insert(case_free_h_.end(), f, f + 5);
 		case_denom_.push_back((0.5 * d.gamma * d.mach * d.mach) * d.cmac);
 		case_aoa_.push_back(d.aoa_deg * 4. * std::atan(1.) / 180);
+		case_ma_h_.push_back((float)d.mach);
+		case_ma_h_.push_back((float)d.aoa_deg);
 	}
 	have_rms0_.assign(ncases_, 0);
 	rms0_.assign(ncases_, {0, 0, 0, 0, 0});
@@ -304,9 +302,24 @@ void Engine::build_blocks(const std::vector<const HostBlock*>& blocks, const std
 	wall_face_.upload(wall_face);
 	roff_d_.upload(roff_);
 	if (ncases_ > 1) {
-		case_free_d_.upload(case_free_h_);
 		gcase_d_.upload(gcase);
 		wall_denom_d_.upload(wall_denom);
+	}
+	case_free_d_.upload(case_free_h_);
+	{  // per-cell and per-case data of the warm-start features
+		std::vector<float> cen(3 * (size_t)NR_);
+		for (int b = 0; b < nb_; b++) {
+			const HostBlock& B = hc.blocks[b];
+			for (int c = 0; c < B.n_real; c++)
+				for (int d = 0; d < 3; d++) cen[3 * (size_t)(roff_[b] + c) + d] = (float)B.cell_center[3 * (size_t)c + d];
+		}
+		cen_d_.upload(cen);
+		block_case_d_.upload(block_case_);
+		std::vector<int> cwo(ncases_ + 1);
+		for (int c = 0; c <= ncases_; c++) cwo[c] = wall_off[case_boff_[c]];
+		case_wall_off_d_.upload(cwo);
+		case_ma_d_.upload(case_ma_h_);
+		fallback_d_.alloc(1);
 	}
 	gkind_.upload(gkind);
 	grefl_.upload(grefl);
@@ -415,6 +428,10 @@ void Engine::init_state() {
 		W0_.upload(W);
 	}
 	cur_ = 0;
+	count_device_bytes();
+}
+
+void Engine::count_device_bytes() {
 	size_t bytes = 0;
 	for (auto* b : {&slot_ptr_, &slot_face_, &slot_nbr_, &slot_mate_, &face_lr_, &halo_dst_, &halo_src_, &wall_off_,
 	                &wall_face_, &roff_d_})
@@ -643,7 +660,7 @@ void Engine::iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* m
 		v.gkind = gkind_.p;
 		v.grefl = grefl_.p;
 		v.W0 = W0_.p;
-		v.case_free = case_free_d_.p;
+		v.case_free = ncases_ > 1 ? case_free_d_.p : nullptr;  // single case: Physics::free
 		v.gcase = gcase_d_.p;
 		if (order_ == 2) {
 			launch_recon<T>(v, ph_, grad_kind_, lim_kind_, s == 0, carry_, st_);
@@ -1266,7 +1283,7 @@ double Engine::run_persistent_t(int iters) {
 		v.gkind = gkind_.p;
 		v.grefl = grefl_.p;
 		v.W0 = W0_.p;
-		v.case_free = case_free_d_.p;
+		v.case_free = ncases_ > 1 ? case_free_d_.p : nullptr;  // single case: Physics::free
 		v.gcase = gcase_d_.p;
 		return v;
 	};
@@ -1468,6 +1485,94 @@ double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch,
 	}
 	std::fill(case_active_.begin(), case_active_.end(), 1);
 	return ms_total;
+}
+
+// ---------------------------------------------------------------- warm start / precision
+void Engine::cell_features(float* dev_out) {
+	launch_cell_features(NR_, nb_, roff_d_.p, block_case_d_.p, cen_d_.p, case_wall_off_d_.p, wall_face_.p, fc_.p,
+	                     case_ma_d_.p, dev_out, st_);
+	check("cell_features");
+}
+
+void Engine::conservative_rows(float* dev_out) {
+	if (opt_.precision == PREC_FP32)
+		launch_prims_to_conservative<float>(NR_, NA_, cur_ ? f32_.P1.p : f32_.P0.p, ph_.gamma, dev_out, st_);
+	else
+		launch_prims_to_conservative<double>(NR_, NA_, cur_ ? f64_.P1.p : f64_.P0.p, ph_.gamma, dev_out, st_);
+	check("conservative_rows");
+}
+
+int Engine::apply_conservative(const float* dev_w, int ld) {
+	if (ld < 5) throw Error(E3D_ERR_ARG, "conservative rows need at least 5 columns");
+	cuda_ok(cudaMemsetAsync(fallback_d_.p, 0, sizeof(int), st_), "memset");
+	if (opt_.precision == PREC_FP32)
+		launch_apply_conservative<float>(NR_, NA_, nb_, roff_d_.p, block_case_d_.p, dev_w, ld, case_free_d_.p,
+		                                 ph_.gamma, f32_.P0.p, f32_.P1.p, carry_ ? W0_.p : nullptr, fallback_d_.p,
+		                                 st_);
+	else
+		launch_apply_conservative<double>(NR_, NA_, nb_, roff_d_.p, block_case_d_.p, dev_w, ld, case_free_d_.p,
+		                                  ph_.gamma, f64_.P0.p, f64_.P1.p, carry_ ? W0_.p : nullptr, fallback_d_.p,
+		                                  st_);
+	check("apply_conservative");
+	int n = 0;
+	cuda_ok(cudaMemcpyAsync(&n, fallback_d_.p, sizeof(int), cudaMemcpyDeviceToHost, st_), "fallback count");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	return n;
+}
+
+void Engine::widen_to_fp64() {
+	if (opt_.precision == PREC_FP64) return;
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	const bool need_gg = order_ == 2 && grad_kind_ == GRAD_GREEN_GAUSS;
+	const bool need_ls = order_ == 2 && grad_kind_ == GRAD_LEAST_SQUARES;
+	f64_.sgeo.alloc(4 * (size_t)NS_);
+	f64_.srv.alloc(3 * (size_t)NS_);
+	if (need_gg) f64_.sS.alloc(3 * (size_t)NS_);
+	launch_slot_geometry64(NS_, slot_face_.p, slot_mate_.p, S_.p, nhat_.p, area_.p, rl_.p, rr_.p, f64_.sgeo.p,
+	                       need_gg ? f64_.sS.p : nullptr, f64_.srv.p, st_);
+	if (need_ls) {
+		f64_.lsw.alloc(lsw64_.n);
+		cuda_ok(cudaMemcpyAsync(f64_.lsw.p, lsw64_.p, lsw64_.n * sizeof(double), cudaMemcpyDeviceToDevice, st_), "lsw");
+	}
+	f64_.vol.alloc(vol64_.n);
+	cuda_ok(cudaMemcpyAsync(f64_.vol.p, vol64_.p, vol64_.n * sizeof(double), cudaMemcpyDeviceToDevice, st_), "vol");
+	f64_.P0.alloc(5 * (size_t)NA_);
+	f64_.P1.alloc(5 * (size_t)NA_);
+	launch_widen_state(NA_, NR_, cur_ ? f32_.P1.p : f32_.P0.p, carry_ ? W0_.p : nullptr, ph_.gm1, f64_.P0.p,
+	                   f64_.P1.p, st_);
+	check("widen");
+	f64_.Rc.alloc(5 * (size_t)NR_);
+	f64_.Rd.alloc(5 * (size_t)NR_);
+	f64_.dt.alloc(NR_);
+	cuda_ok(cudaMemsetAsync(f64_.Rc.p, 0, f64_.Rc.n * sizeof(double), st_), "memset");
+	cuda_ok(cudaMemsetAsync(f64_.Rd.p, 0, f64_.Rd.n * sizeof(double), st_), "memset");
+	cuda_ok(cudaMemsetAsync(f64_.dt.p, 0, f64_.dt.n * sizeof(double), st_), "memset");
+	f64_.FS.alloc(order_ == 2 ? 5 * (size_t)NS_ : 0);
+	srad_.alloc(NR_);
+	grad_.alloc(15 * (size_t)NA_);
+	lim_.alloc(5 * (size_t)NA_);
+	cuda_ok(cudaMemsetAsync(srad_.p, 0, srad_.n * sizeof(double), st_), "memset");
+	cuda_ok(cudaMemsetAsync(grad_.p, 0, grad_.n * sizeof(double), st_), "memset");
+	cuda_ok(cudaMemsetAsync(lim_.p, 0, lim_.n * sizeof(double), st_), "memset");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	for (auto* b : {&f32_.P0, &f32_.P1, &f32_.FS, &f32_.Rc, &f32_.Rd, &f32_.dt, &f32_.sgeo, &f32_.sS, &f32_.srv,
+	                &f32_.lsw, &f32_.vol})
+		b->free();
+	cur_ = 0;
+	opt_.precision = PREC_FP64;
+	for (auto& g : graph_)
+		if (g) {
+			cudaGraphExecDestroy(g);
+			g = nullptr;
+		}
+	if (pgraph_) {
+		cudaGraphExecDestroy(pgraph_);
+		pgraph_ = nullptr;
+	}
+	grid_ = 0;
+	tuning_ = Tuning{};
+	snap_.free();
+	count_device_bytes();
 }
 
 }  // namespace e3d

@@ -31,6 +31,10 @@ struct IterRecord {
 	double cl, cd, cmx, cmy, cmz;
 };
 
+inline void cuda_ok(cudaError_t e, const char* what) {
+	if (e != cudaSuccess) throw Error(E3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
 template <class T>
 struct DevBuf {
 	T* p = nullptr;
@@ -94,6 +98,19 @@ public:
 	const std::vector<IterRecord>& history() const { return hist_case_[0]; }
 	const std::vector<IterRecord>& history(int c) const { return hist_case_.at(c); }
 	int n_cases() const { return ncases_; }
+
+	// --- warm start and precision switch (batched / learned forms)
+	// raw surrogate inputs of every real cell, [NR][8] floats on the device:
+	// centroid x y z, distance to the nearest wall-face centre of the cell's case, Mach, alpha (deg), 0, 0
+	void cell_features(float* dev_out);
+	// conservative state of every real cell, [NR][8] floats on the device (5 used)
+	void conservative_rows(float* dev_out);
+	// writes a conservative state ([NR][ld] floats on the device) into every real cell; cells whose
+	// prediction is not physical keep the freestream state of their case; returns how many did
+	int apply_conservative(const float* dev_w, int ld);
+	// FP32 solver -> FP64 solver in place: FP64 geometry and state (real cells from the carried FP64
+	// conservative state), histories and reference norms kept, FP32 buffers released
+	void widen_to_fp64();
 	long long n_real_case(int c) const;
 	void sync();  // waits for queued work; throws on a CUDA error or a non-finite norm
 
@@ -133,6 +150,7 @@ private:
 	void setup(const std::vector<const HostCase*>& cases);
 	void build_blocks(const std::vector<const HostBlock*>& blocks, const std::vector<Connexion>& conns);
 	void init_state();
+	void count_device_bytes();
 	void check(const char* what);
 	template <class T>
 	void iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* marks);
@@ -158,6 +176,9 @@ private:
 	std::vector<int> block_case_;     // case of each block
 	std::vector<double> case_free_h_, case_denom_, case_aoa_;
 	DevBuf<double> case_free_d_, wall_denom_d_;
+	std::vector<float> case_ma_h_;        // Mach, alpha (deg) of each case
+	DevBuf<float> cen_d_, case_ma_d_;     // real-cell centroids [NR][3]; per-case Mach/alpha
+	DevBuf<int> block_case_d_, case_wall_off_d_, fallback_d_;
 	DevBuf<int> gcase_d_;
 	int carry_ = 0;
 	int grad_kind_ = GRAD_LEAST_SQUARES, lim_kind_ = LIM_VENKATAKRISHNAN, scheme_ = FLUX_ROE, order_ = 1;

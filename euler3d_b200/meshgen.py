@@ -60,8 +60,8 @@ class BumpChannel:
     node_ijk: np.ndarray  # (P, 3) integer lattice coordinates
 
 
-def bump_channel(n: int, height: float = 0.05, sigma: float = 0.1) -> BumpChannel:
-    """Build the n x n x n hexahedron box [0,1]^3 split into 6 n^3 tetrahedra."""
+def bump_channel(n: int, height: float = 0.05, sigma: float = 0.1, ytop: float = 1.0) -> BumpChannel:
+    """Build the n x n x n hexahedron box [0,1] x [0,ytop] x [0,1] split into 6 n^3 tetrahedra."""
     m = n + 1
     ii, jj, kk = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
     # node id = i + m*(j + m*k)  (x fastest)
@@ -70,8 +70,10 @@ def bump_channel(n: int, height: float = 0.05, sigma: float = 0.1) -> BumpChanne
     x = ijk[:, 0] / n
     y = ijk[:, 1] / n
     z = ijk[:, 2] / n
+    if ytop != 1.0:
+        y = y * ytop
     h = height * np.exp(-((x - 0.5) ** 2) / (2.0 * sigma * sigma))
-    y = y + h * (1.0 - y)
+    y = y + h * (1.0 - y / ytop)
     nodes = np.stack([x, y, z], axis=1)
 
     hi, hj, hk = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
@@ -107,11 +109,17 @@ class BlockMesh:
         return int(sum(len(f) for t, f in self.markers if t != "CONNEXION"))
 
 
-def slab_blocks(mesh: BumpChannel, n_blocks: int = 1) -> list[BlockMesh]:
+def slab_blocks(mesh: BumpChannel, n_blocks: int = 1, sides: str = "farfield") -> list[BlockMesh]:
     """Cut the channel into ``n_blocks`` x-slabs of whole hexahedron layers.
 
     Every block lists WALL (y=0) then FARFIELD (other outer sides) then one
-    CONNEXION marker per neighbouring slab (lower x first).  Ghost elements of a
+    CONNEXION marker per neighbouring slab (lower x first).  With
+    ``sides="symmetry"`` the z=0 and z=1 planes form a SYMMETRY marker (after
+    FARFIELD) instead of being farfield, and with ``sides="channel"`` the top
+    plane joins them: the inlet and outlet are then the only farfield faces.
+    Farfield faces the flow runs along switch between the inflow and outflow
+    states with the sign of u.n, which keeps the residual from dropping below
+    a few orders; a channel has none.  Ghost elements of a
     marker follow ascending (owner cell, local face).  The connexion origin ids
     are the neighbour block's local cell ids across each interface face, in the
     same order, which is what the topology file records.
@@ -131,12 +139,24 @@ def slab_blocks(mesh: BumpChannel, n_blocks: int = 1) -> list[BlockMesh]:
         return np.where(lo == v.max(axis=1), lo, -1)
 
     px, py, pz = plane(0), plane(1), plane(2)
+    if sides not in ("farfield", "symmetry", "channel"):
+        raise ValueError(f"sides must be 'farfield', 'symmetry' or 'channel', not {sides!r}")
     wall = py == 0
-    far = (px == 0) | (px == n) | (py == n) | (pz == 0) | (pz == n)
+    zside = (pz == 0) | (pz == n)
+    top = py == n
+    far = (px == 0) | (px == n)
+    if sides == "farfield":
+        far = far | top | zside
+        sym = np.zeros_like(far)
+    elif sides == "symmetry":
+        far = far | top
+        sym = zside & ~far
+    else:
+        sym = (zside | top) & ~far
     iface = (px > 0) & (px < n) & (px % layers == 0)
-    keep = np.nonzero(wall | far | iface)[0]  # small: only faces on planes of interest
+    keep = np.nonzero(wall | far | sym | iface)[0]  # small: only faces on planes of interest
     faces, owner = faces[keep], owner[keep]
-    wall, far, iface, px = wall[keep], far[keep], iface[keep], px[keep]
+    wall, far, sym, iface, px = wall[keep], far[keep], sym[keep], iface[keep], px[keep]
 
     tet_block = mesh.hex_i // layers
     local_id = np.empty(n_tets, dtype=np.int64)
@@ -171,6 +191,8 @@ def slab_blocks(mesh: BumpChannel, n_blocks: int = 1) -> list[BlockMesh]:
         in_b = fblock == b
         blk.markers.append(("WALL", g2l[faces[in_b & wall]]))
         blk.markers.append(("FARFIELD", g2l[faces[in_b & far]]))
+        if sides != "farfield":
+            blk.markers.append(("SYMMETRY", g2l[faces[in_b & sym]]))
         for nb, pl in ((b - 1, b * layers), (b + 1, (b + 1) * layers)):
             if nb < 0 or nb >= n_blocks:
                 continue
@@ -352,7 +374,8 @@ def write_hex_case(directory: str, n: int, nz: int = 1, prefix: str = "hexchan",
 
 
 def write_case(directory: str, n: int, n_blocks: int = 1, prefix: str = "bump",
-               deck: Deck | None = None, height: float = 0.05, sigma: float = 0.1) -> str:
+               deck: Deck | None = None, height: float = 0.05, sigma: float = 0.1, sides: str = "farfield",
+               ytop: float = 1.0) -> str:
     """Generate a bump-channel case in ``directory``; return the deck path.
 
     File names inside the topology and deck are relative, so the case runs
@@ -360,8 +383,8 @@ def write_case(directory: str, n: int, n_blocks: int = 1, prefix: str = "bump",
     relative to its CWD).
     """
     os.makedirs(directory, exist_ok=True)
-    mesh = bump_channel(n, height=height, sigma=sigma)
-    blocks = slab_blocks(mesh, n_blocks)
+    mesh = bump_channel(n, height=height, sigma=sigma, ytop=ytop)
+    blocks = slab_blocks(mesh, n_blocks, sides)
     files = []
     for b, blk in enumerate(blocks):
         name = f"{prefix}_B{b}.su2" if n_blocks > 1 else f"{prefix}.su2"

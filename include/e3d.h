@@ -170,6 +170,47 @@ int e3d_case_history_length(const e3d_solver* s, int case_index, int* n);
 int e3d_case_history(const e3d_solver* s, int case_index, int first, int count, e3d_iter_record* out);
 int e3d_batch_tuning(const e3d_solver* s, int* tile_cells, int* grid, double* ms_per_iter, int* from_cache);
 
+/* ---- precision switch, warm start and the learned surrogate -------------------
+ * No counterpart in the reference.
+ * e3d_solver_set_precision: an FP32 solver becomes an FP64 solver in place
+ * (E3D_FP64 only); real cells take the carried FP64 conservative state,
+ * histories and the iteration-0 reference norms carry on.  The FP32 path's
+ * residual stops dropping near 5 orders (FP32 rounding of the fluxes); a run
+ * to a deeper drop continues in FP64 from there.
+ * e3d_cell_features: surrogate inputs of every real cell of every case, in
+ * device cell order (blocks in order, real cells in file order), 8 floats per
+ * cell: centroid x y z, distance to the nearest wall-face centre of the
+ * cell's case, Mach, alpha (deg), 0, 0.
+ * The surrogate is a 4-layer MLP 6 -> 128 -> 128 -> 128 -> 5 with exact-erf
+ * GELU, BF16 weights and FP32 accumulation on the tensor cores, trained by its
+ * own forward/backward kernels and Adam on FP32 master weights (deterministic:
+ * no floating-point atomics).  Samples: features (6 per row, as above) and the
+ * converged conservative state (rho, rho u, rho v, rho w, rho E; 5 per row).
+ * e3d_warm_start writes the predicted state into every real cell of every case
+ * of a solver; cells whose prediction is not physical keep the freestream
+ * start (*n_fallback counts them).  Call it after one iteration from the
+ * freestream start so the residual drop is measured from the same reference
+ * norm as a plain start's. */
+int e3d_solver_set_precision(e3d_solver* s, int precision);
+int e3d_cell_features(e3d_solver* s, float* out, int64_t n_floats);
+
+typedef struct e3d_surrogate e3d_surrogate;
+#define E3D_SURROGATE_PARAMS 36232 /* flat FP32 parameter count (padded layers) */
+#define E3D_SURROGATE_NORM 24      /* feature mean[8], feature std[8], target scale[8] */
+int e3d_surrogate_create(int device, uint64_t seed, double gamma, e3d_surrogate** out);
+int e3d_surrogate_free(e3d_surrogate* m);
+int e3d_surrogate_add_solution(e3d_surrogate* m, e3d_solver* s);
+int e3d_surrogate_add_samples(e3d_surrogate* m, const float* features6, const float* states5, int64_t n);
+int e3d_surrogate_sample_count(const e3d_surrogate* m, int64_t* n);
+int e3d_surrogate_clear(e3d_surrogate* m);
+int e3d_surrogate_train(e3d_surrogate* m, int steps, int batch, double lr, float* loss_per_step, double* final_loss);
+int e3d_surrogate_gradient(e3d_surrogate* m, const float* features6, const float* states5, int n, float* grad,
+                           double* loss);
+int e3d_surrogate_predict(e3d_surrogate* m, const float* features6, int64_t n, float* states5);
+int e3d_surrogate_get_params(const e3d_surrogate* m, float* params, float* norm);
+int e3d_surrogate_set_params(e3d_surrogate* m, const float* params, const float* norm);
+int e3d_warm_start(e3d_solver* s, e3d_surrogate* m, int* n_fallback);
+
 /* Checkpoint / restart of the whole solver state (the reference's restart
  * writer is an empty stub, PostProcessing/src/OutputTecplot.cpp:475-494):
  * current primitives of every cell in the solver precision, the FP64
