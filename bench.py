@@ -219,6 +219,147 @@ def combine_ranks(local_ms: float, cells: int, steps: int, world: int, dist=None
 
 
 # ------------------------------------------------------------------ our arm
+# ------------------------------------------------------------------ sweep workloads
+POLAR_SCHEME = dict(order=2, flux="ausm", gradient="greengauss", limiter="barthjespersen", omega=2.16e-16, stages=5,
+                    cfl=1.5)
+WARM_SCHEME = dict(order=1, flux="ausm", stages=5, cfl=1.5)
+
+
+def _ref_sample(decks, iters, procs):
+    """The reference solver (oracle driver, fast face builder) on `procs`
+    cases at once, `iters` iterations each: aggregate cell-iterations/s."""
+    if not os.path.exists(REFDRIVER):
+        return None
+    jobs = []
+    t0 = time.perf_counter()
+    for d in decks[:procs]:
+        jobs.append(subprocess.Popen([REFDRIVER, os.path.basename(d), "--iters", str(iters), "--warmup", "0",
+                                      "--blocks", "0:1", "--quiet"],
+                                     cwd=os.path.dirname(d), stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                     text=True))
+    total = 0.0
+    slow = 0.0
+    for j in jobs:
+        out, _ = j.communicate()
+        r = json.loads(out.strip().splitlines()[-1])
+        total += r["cells"] * r["iters"]
+        slow = max(slow, r["solve_s"])
+    return {"value": total / slow, "unit": UNIT, "cores": len(jobs), "kind": "reference",
+            "sample": f"{len(jobs)} cases of the sweep run concurrently (one process and core each), {iters} "
+                      f"iterations each, reference solver compiled from its sources (-O2, fast face builder); "
+                      f"aggregate = sum(cells x iterations) / slowest solve time",
+            "wall_s": time.perf_counter() - t0}
+
+
+def run_sweep_workload(a, rank, world):
+    import torch
+
+    from euler3d_b200 import api
+    from euler3d_b200 import sweep as sw
+
+    if world > 1 and rank != 0:
+        return 0  # the sweep workloads are single-GPU measurements
+    torch.cuda.set_device(0)
+    small = a.scale == "small"
+    nr = (10, 16) if small else (25, 60)
+    clocks = ClockSampler(0)
+    with tempfile.TemporaryDirectory() as td:
+        if a.workload == "polar":
+            specs = sw.polar_specs(3, 16 if small else 64, n_range=nr)
+            t0 = time.time()
+            decks = sw.write_cases(td, specs, POLAR_SCHEME, sides="farfield")
+            cases = [api.Case(d) for d in decks]
+            log(f"[bench] {len(cases)} cases written and loaded in {time.time() - t0:.1f}s")
+            cells = sum(c.block_info(0).n_real for c in cases)
+            warm, steps = max(3, a.warmup), max(1, a.steps)
+            forms = {}
+            for form in ("persistent", "per-pass", None):
+                if form:
+                    os.environ["E3D_BATCH_FORM"] = form
+                else:
+                    os.environ.pop("E3D_BATCH_FORM", None)
+                b = api.Batch(cases, precision="fp32", hist_capacity=max(4096, warm + steps + 64))
+                b.solve_batch(warm, -1e300, iters_per_launch=warm)  # autotune + warm-up iterations
+                torch.cuda.synchronize()
+                if form is None:
+                    clocks.mark("start")
+                _, ms = b.solve_batch(warm + steps, -1e300, iters_per_launch=steps)
+                if form is None:
+                    clocks.mark("end")
+                forms[form or "autotuned"] = {"value": cells * steps / (ms / 1e3), "ms": ms, "tuning": b.tuning()}
+                b.close()
+            value, ms = forms["autotuned"]["value"], forms["autotuned"]["ms"]
+            # plain: the same iterations case after case through the single-case path
+            plain = {}
+            for prec in ("fp32", "fp64"):
+                tot = 0.0
+                for c in cases:
+                    s = api.Solver(c, precision=prec)
+                    s.iterate(warm)
+                    tot += s.iterate_timed(steps)
+                    s.close()
+                plain[prec] = {"value": cells * steps / (tot / 1e3), "ms": tot}
+            cpu = None if a.no_cpu_baseline else _ref_sample(
+                sorted(decks, key=lambda d: os.path.getsize(d.replace(".deck", ".su2"))), 2,
+                min(len(decks), os.cpu_count() or 1))
+            line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warm,
+                    "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "f32", "data": "synthetic",
+                    "config": {"workload": f"polar sweep: {len(cases)} bump channels n~U{{{nr[0]}..{nr[1]}}} "
+                                           f"(seed 3), Mach U[0.3,0.8], alpha U[-2,6]; AUSM + Green-Gauss + "
+                                           f"Barth-Jespersen, order 2, 5-stage RK, CFL 1.5; all cases in one "
+                                           f"batch, form and tiles autotuned",
+                               "cells": cells, "cases": len(cases),
+                               "arithmetic": "fp32 fluxes/gradients/limiters, fp64 conserved state and reductions",
+                               "l2": "working set far larger than the 126 MB L2"},
+                    "forms": forms, "plain_per_case": plain, "batched_vs_plain_fp32": value / plain["fp32"]["value"],
+                    "batched_vs_plain_fp64": value / plain["fp64"]["value"], "cpu_baseline": cpu,
+                    "clocks": ClockSampler.summarize(clocks.stop())}
+        else:
+            t0 = time.time()
+            tr_specs = sw.polar_specs(1000, 24 if small else 200, n_range=nr, prefix="train")
+            te_specs = sw.polar_specs(2000, 8 if small else 32, n_range=nr, prefix="test")
+            decks = sw.write_cases(td, tr_specs + te_specs, WARM_SCHEME, sides="channel")
+            cases = [api.Case(d) for d in decks]
+            train, test = cases[:len(tr_specs)], cases[len(tr_specs):]
+            log(f"[bench] {len(cases)} cases written and loaded in {time.time() - t0:.1f}s")
+            crit, max_iter = -8.0, 200000
+            m, tinfo = sw.train_surrogate(train, seed=1000, criterion=-4.0, steps=6000 if not small else 3000)
+            log(f"[bench] surrogate: {tinfo}")
+            clocks.mark("start")
+            learned = sw.solve_batched(test, crit, max_iter, surrogate=m)
+            log(f"[bench] batched + learned: {learned['wall_s']:.2f}s {learned['phases']}")
+            batched = sw.solve_batched(test, crit, max_iter, surrogate=None)
+            log(f"[bench] batched: {batched['wall_s']:.2f}s {batched['phases']}")
+            plain = []
+            for c in test:
+                plain.append(sw.solve_plain(c, crit, max_iter))
+                log(f"[bench] plain case {len(plain)}: {plain[-1]}")
+            clocks.mark("end")
+            t_plain = sum(p["wall_s"] for p in plain)
+            cells = sum(p["cells"] for p in plain)
+            dcl = max(abs(l["cl"] - p["cl"]) / max(abs(p["cl"]), 1e-2) for l, p in zip(learned["cases"], plain))
+            dcd = max(abs(l["cd"] - p["cd"]) / max(abs(p["cd"]), 1e-2) for l, p in zip(learned["cases"], plain))
+            line = {"metric": "time to 1e-8 density-residual drop (s)", "value": learned["wall_s"], "unit": "s",
+                    "n_gpus": 1, "steps": len(test), "warmup": 0, "ms_per_step": None, "higher_is_better": False,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+                    "config": {"workload": f"{len(test)} held-out channel cases n~U{{{nr[0]}..{nr[1]}}} (seed 2000), "
+                                           f"Mach U[0.3,0.8], alpha U[-2,6], first-order AUSM, 5-stage RK, CFL 1.5; "
+                                           f"surrogate trained on {len(train)} cases (seed 1000)",
+                               "cells": cells, "criterion": crit},
+                    "plain_s": t_plain, "batched_s": batched["wall_s"], "speedup_learned": t_plain / learned["wall_s"],
+                    "speedup_batched_only": t_plain / batched["wall_s"],
+                    "iters_plain": [p["reached"] for p in plain],
+                    "iters_learned": [c["reached"] for c in learned["cases"]],
+                    "iters_batched": [c["reached"] for c in batched["cases"]],
+                    "max_rel_dcl": dcl, "max_rel_dcd": dcd,
+                    "learned": {k: v for k, v in learned.items() if k != "cases"},
+                    "batched": {k: v for k, v in batched.items() if k != "cases"},
+                    "surrogate": tinfo, "clocks": ClockSampler.summarize(clocks.stop())}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,12 +371,19 @@ def main():
     ap.add_argument("--blocks", type=int, default=WORKLOAD["blocks"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["channel", "polar", "warmstart"], default="channel",
+                    help="channel: the 3.07M-tet second-order case (default); polar: 64-case batched sweep "
+                         "throughput; warmstart: time to an 8-order drop, batched + learned vs plain")
+    ap.add_argument("--scale", choices=["full", "small"], default="full",
+                    help="small: the same sweep workloads on 10^3..16^3 meshes (quick checks)")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return run_reference_arm(a, rank)
+    if a.workload != "channel":
+        return run_sweep_workload(a, rank, world)
 
     import torch
     import torch.distributed as dist

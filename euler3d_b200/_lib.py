@@ -97,7 +97,8 @@ SIGNATURES = {
                           C.POINTER(C.c_int)], C.c_int),
     "e3d_launches_per_iteration": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "e3d_batch_create": ([C.c_void_p, C.c_int, C.POINTER(Options), C.POINTER(C.c_void_p)], C.c_int),
-    "e3d_batch_solve": ([C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_void_p, C.POINTER(C.c_double)], C.c_int),
+    "e3d_batch_solve": ([C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double)],
+                        C.c_int),
     "e3d_case_count": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "e3d_case_history_length": ([C.c_void_p, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "e3d_case_history": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),

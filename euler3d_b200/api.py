@@ -225,11 +225,12 @@ class Batch(Solver):
         self.n_blocks = sum(c.n_blocks for c in cases)
         self._info = [c.block_info(b) for c in cases for b in range(c.n_blocks)]
 
-    def solve_batch(self, max_iter: int, criterion: float, iters_per_launch: int = 10):
+    def solve_batch(self, max_iter: int, criterion: float, iters_per_launch: int = 10, stall_window: int = 0):
         """Returns (iterations needed per case, device ms of the whole solve)."""
         done = np.zeros(len(self.cases), dtype=np.int32)
         ms = C.c_double()
-        L.check(L.lib().e3d_batch_solve(self._h, max_iter, criterion, iters_per_launch, L.ptr(done), C.byref(ms)))
+        L.check(L.lib().e3d_batch_solve(self._h, max_iter, criterion, iters_per_launch, stall_window, L.ptr(done),
+                                        C.byref(ms)))
         return done, ms.value
 
     def case_history(self, c: int) -> dict[str, np.ndarray]:
@@ -247,7 +248,8 @@ class Batch(Solver):
     def tuning(self) -> dict:
         t, g, ms, fc = C.c_int(), C.c_int(), C.c_double(), C.c_int()
         L.check(L.lib().e3d_batch_tuning(self._h, C.byref(t), C.byref(g), C.byref(ms), C.byref(fc)))
-        return {"tile_cells": t.value, "grid": g.value, "ms_per_iter": ms.value, "from_cache": bool(fc.value)}
+        return {"tile_cells": t.value, "grid": g.value, "mode": "per-pass" if g.value == 0 else "persistent",
+                "ms_per_iter": ms.value, "from_cache": bool(fc.value)}
 
 
 def set_precision(solver: Solver, precision: str) -> None:

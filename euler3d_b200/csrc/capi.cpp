@@ -244,11 +244,11 @@ int e3d_batch_create(const e3d_case* const* cases, int n_cases, const e3d_option
 	});
 }
 
-int e3d_batch_solve(e3d_solver* s, int max_iter, double criterion, int iters_per_launch, int* iters_done,
-                    double* device_ms) {
+int e3d_batch_solve(e3d_solver* s, int max_iter, double criterion, int iters_per_launch, int stall_window,
+                    int* iters_done, double* device_ms) {
 	return guard([&] {
 		std::vector<int> done;
-		const double ms = eng(s).solve_batch(max_iter, criterion, iters_per_launch, done);
+		const double ms = eng(s).solve_batch(max_iter, criterion, iters_per_launch, stall_window, done);
 		if (iters_done)
 			for (size_t i = 0; i < done.size(); i++) iters_done[i] = done[i];
 		if (device_ms) *device_ms = ms;

@@ -1288,22 +1288,26 @@ double Engine::run_persistent_t(int iters) {
 		return v;
 	};
 	const FusedView<T> v0 = view(false), v1 = view(true);
-	const int grid = std::max(1, std::min(grid_, n_work_));
+	const int grid = tiled_ ? n_work_ : std::max(1, std::min(grid_, n_work_));
+	auto launch = [&]() {
+		return tiled_ ? launch_tiled_iterations<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, order_ == 2, st_)
+		              : launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, order_ == 2, grid, st_);
+	};
 	cudaEvent_t e0, e1;
 	cuda_ok(cudaEventCreate(&e0), "event");
 	cuda_ok(cudaEventCreate(&e1), "event");
 	cuda_ok(cudaEventRecord(e0, st_), "event");
 	bool launched = false;
 	if (opt_.use_graph) {
-		if (pgraph_ && (pgraph_iters_ != iters || pgraph_parity_ != cur_ || pgraph_grid_ != grid)) {
+		if (pgraph_ && (pgraph_iters_ != iters || pgraph_parity_ != cur_ || pgraph_grid_ != grid ||
+		                pgraph_tiled_ != tiled_)) {
 			cudaGraphExecDestroy(pgraph_);
 			pgraph_ = nullptr;
 		}
 		if (!pgraph_) {
 			cudaGraph_t g;
 			if (cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-				const cudaError_t le =
-				    launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, order_ == 2, grid, st_);
+				const cudaError_t le = launch();
 				const cudaError_t ce = cudaStreamEndCapture(st_, &g);
 				if (le == cudaSuccess && ce == cudaSuccess) {
 					if (cudaGraphInstantiate(&pgraph_, g, 0) != cudaSuccess) pgraph_ = nullptr;
@@ -1316,6 +1320,7 @@ double Engine::run_persistent_t(int iters) {
 			pgraph_iters_ = iters;
 			pgraph_parity_ = cur_;
 			pgraph_grid_ = grid;
+			pgraph_tiled_ = tiled_;
 		}
 		if (pgraph_) {
 			cuda_ok(cudaGraphLaunch(pgraph_, st_), "graph launch");
@@ -1323,9 +1328,7 @@ double Engine::run_persistent_t(int iters) {
 			tuning_.graph = true;
 		}
 	}
-	if (!launched)
-		cuda_ok(launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, order_ == 2, grid, st_),
-		        "cooperative launch");
+	if (!launched) cuda_ok(launch(), tiled_ ? "tiled launch" : "cooperative launch");
 	cuda_ok(cudaEventRecord(e1, st_), "event");
 	cuda_ok(cudaEventSynchronize(e1), "event sync");
 	float ms = 0.f;
@@ -1380,13 +1383,19 @@ void Engine::autotune(int iters) {
 	int bucket = 0;
 	while ((1LL << bucket) < (long long)NR_) bucket++;
 	const TuneKey key{bucket, scheme_, grad_kind_, lim_kind_, order_ + 4 * (int)opt_.precision};
-	auto it = g_tune.find(key);
-	if (it != g_tune.end()) {
+	// E3D_BATCH_FORM=persistent or per-pass restricts the search (and bypasses the cache)
+	const char* form_env = std::getenv("E3D_BATCH_FORM");
+	const std::string form = form_env ? form_env : "";
+	const bool only_tiled = form == "per-pass", only_persistent = form == "persistent";
+	auto it = (only_tiled || only_persistent) ? g_tune.end() : g_tune.find(key);
+	if (it != g_tune.end()) {  // blocks per SM 0: the tiled per-pass form
 		tile_mult_ = it->second.first;
-		grid_ = std::min(maxb, it->second.second) * sms;
+		tiled_ = it->second.second == 0;
+		grid_ = tiled_ ? sms : std::min(maxb, it->second.second) * sms;
 		build_work();
 		tuning_.tile_cells = tile_mult_ * kPersistThreads;
-		tuning_.grid = grid_;
+		tuning_.grid = tiled_ ? 0 : grid_;
+		tuning_.tiled = tiled_;
 		tuning_.from_cache = true;
 		return;
 	}
@@ -1398,8 +1407,12 @@ void Engine::autotune(int iters) {
 	for (int tm : {1, 2, 4}) {
 		tile_mult_ = tm;
 		build_work();
-		for (int b = maxb; b >= 1; b = b > 2 ? b - 2 : b - 1) {
-			grid_ = b * sms;
+		// b = 0: the tiled per-pass form (one 128-cell tile per block); b > 0: the persistent kernel
+		// with b blocks per SM
+		for (int b = maxb; b >= (tm == 1 ? 0 : 1); b = b > 2 ? b - 2 : b - 1) {
+			if ((only_tiled && b > 0) || (only_persistent && b == 0)) continue;
+			tiled_ = b == 0;
+			grid_ = tiled_ ? sms : b * sms;
 			run_persistent(1);  // warm (and capture)
 			const double ms = run_persistent(iters) / iters;
 			if (ms < best) {
@@ -1413,17 +1426,22 @@ void Engine::autotune(int iters) {
 		}
 	}
 	tile_mult_ = best_tm;
-	grid_ = best_b * sms;
+	tiled_ = best_b == 0;
+	grid_ = tiled_ ? sms : best_b * sms;
 	build_work();
-	g_tune[key] = {best_tm, best_b};
-	tune_cache_store();
+	if (!only_tiled && !only_persistent) {
+		g_tune[key] = {best_tm, best_b};
+		tune_cache_store();
+	}
 	tuning_.tile_cells = best_tm * kPersistThreads;
-	tuning_.grid = grid_;
+	tuning_.grid = tiled_ ? 0 : grid_;
+	tuning_.tiled = tiled_;
 	tuning_.ms_per_iter = best;
 	tuning_.from_cache = false;
 }
 
-double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch, std::vector<int>& iters_done) {
+double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch, int stall_window,
+                           std::vector<int>& iters_done) {
 	if (iters_per_launch < 1) iters_per_launch = 1;
 	if (!started_) halo();
 	collect_history(total_iter_, dev_iter_);
@@ -1434,12 +1452,20 @@ double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch,
 		for (int c = 0; c < ncases_; c++) {
 			if (!case_active_[c]) continue;
 			const auto& h = hist_case_[c];
-			for (const IterRecord& r : h)
-				if (r.conv[0] <= criterion || (int)h.size() >= max_iter) {
-					case_active_[c] = 0;
-					changed = true;
-					break;
-				}
+			bool stop = (int)h.size() >= max_iter;
+			for (const IterRecord& r : h) stop = stop || r.conv[0] <= criterion;
+			if (!stop && stall_window > 0 && (int)h.size() >= 2 * stall_window) {
+				// stalled: the last window brought no new minimum deeper by 0.05 decades
+				const size_t split = h.size() - (size_t)stall_window;
+				double before = 1e300, recent = 1e300;
+				for (size_t i = 0; i < split; i++) before = std::min(before, h[i].conv[0]);
+				for (size_t i = split; i < h.size(); i++) recent = std::min(recent, h[i].conv[0]);
+				stop = recent > before - 0.05;
+			}
+			if (stop) {
+				case_active_[c] = 0;
+				changed = true;
+			}
 		}
 		return changed;
 	};

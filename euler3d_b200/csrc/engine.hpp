@@ -87,11 +87,12 @@ public:
 	// kernel (FP32); a case stops (its tiles leave the work list) once its
 	// density drop reaches `criterion` or it has run max_iter iterations.
 	// iters_done[c] = iterations case c ran.  Returns the device time in ms.
-	double solve_batch(int max_iter, double criterion, int iters_per_launch, std::vector<int>& iters_done);
+	double solve_batch(int max_iter, double criterion, int iters_per_launch, int stall_window,
+	                   std::vector<int>& iters_done);
 	struct Tuning {
 		int tile_cells = 0, grid = 0;
 		double ms_per_iter = 0.0;
-		bool from_cache = false, graph = false;
+		bool from_cache = false, graph = false, tiled = false;
 	};
 	const Tuning& tuning() const { return tuning_; }
 
@@ -212,6 +213,7 @@ private:
 	Tuning tuning_;
 	cudaGraphExec_t pgraph_ = nullptr;
 	int pgraph_iters_ = 0, pgraph_parity_ = -1, pgraph_grid_ = 0;
+	bool tiled_ = false, pgraph_tiled_ = false;
 	void build_work();
 	double run_persistent(int iters);
 	template <class T>

@@ -14,4 +14,7 @@ template int persistent_blocks_per_sm<float>(int, int, int, bool);
 template cudaError_t launch_persistent<float>(const FusedView<float>&, const FusedView<float>&, const Physics&,
                                               const PersistArgs&, int, int, int, bool, int, cudaStream_t);
 
+template cudaError_t launch_tiled_iterations<float>(const FusedView<float>&, const FusedView<float>&, const Physics&,
+                                                    const PersistArgs&, int, int, int, bool, cudaStream_t);
+
 }  // namespace e3d

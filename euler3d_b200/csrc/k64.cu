@@ -68,4 +68,7 @@ template int persistent_blocks_per_sm<double>(int, int, int, bool);
 template cudaError_t launch_persistent<double>(const FusedView<double>&, const FusedView<double>&, const Physics&,
                                                const PersistArgs&, int, int, int, bool, int, cudaStream_t);
 
+template cudaError_t launch_tiled_iterations<double>(const FusedView<double>&, const FusedView<double>&, const Physics&,
+                                                    const PersistArgs&, int, int, int, bool, cudaStream_t);
+
 }  // namespace e3d

@@ -782,13 +782,102 @@ __global__ void __launch_bounds__(128) k_wall_sums(const double* __restrict__ te
 __global__ void k_iter_advance(int* d_iter) { *d_iter += 1; }
 
 
-// ===================================================================== persistent
-// Batched cases: one cooperative launch runs `iters` outer iterations over the
-// work list.  Phases are separated by grid-wide barriers: per stage the
-// reconstruction pass and the flux/update pass (the same per-cell functions as
-// the one-kernel-per-pass path), then per iteration the norm partials, wall
-// terms and halo, then the per-block sums into the history.  Tiles of
-// converged cases are simply absent from the work list.
+// ===================================================================== batches
+// Phases of one outer iteration over a work list (tiles of real cells of the
+// active cases), shared by the persistent kernel and the tiled per-pass
+// kernels.  TPB threads cooperate on one tile.
+
+// Sum of (Rc-Rd)^2 over the cells of tile w, fixed tree order (red: [5][TPB]).
+template <class T, int TPB>
+__device__ __forceinline__ void tile_norms(const FusedView<T>& vf, const PersistArgs& a, int w, double (*red)[TPB]) {
+	const int4 t = a.work[w];
+	double acc[5] = {0., 0., 0., 0., 0.};
+	for (int c = t.x + threadIdx.x; c < t.y; c += TPB)
+		for (int q = 0; q < 5; q++) {
+			const double r = (double)vf.Rc[q * vf.NR + c] - (double)vf.Rd[q * vf.NR + c];
+			acc[q] += r * r;
+		}
+	for (int q = 0; q < 5; q++) red[q][threadIdx.x] = acc[q];
+	__syncthreads();
+	for (int h = TPB / 2; h > 0; h >>= 1) {
+		if (threadIdx.x < h)
+			for (int q = 0; q < 5; q++) red[q][threadIdx.x] += red[q][threadIdx.x + h];
+		__syncthreads();
+	}
+	if (threadIdx.x < 5) a.wpart[(size_t)w * 5 + threadIdx.x] = red[threadIdx.x][0];
+	__syncthreads();
+}
+
+// Force terms of wall faces i0, i0+stride, ... (frozen cases included: cheap, ignored by the host).
+template <class T>
+__device__ __forceinline__ void wall_terms_range(const FusedView<T>& vf, const PersistArgs& a, int i0, int stride) {
+	for (int i = i0; i < a.n_wall; i += stride) {
+		const int f = a.wall_face[i];
+		const double p0 = (double)vf.Pin[4 * (size_t)vf.NA + a.face_lr[2 * f]];
+		const double p1 = (double)vf.Pin[4 * (size_t)vf.NA + a.face_lr[2 * f + 1]];
+		const double cp = (0.5 * (p0 + p1) - 1.) / (a.wall_denom ? a.wall_denom[i] : a.denom);
+		const double fx = cp * a.S[3 * f], fy = cp * a.S[3 * f + 1], fz = cp * a.S[3 * f + 2];
+		const double x = a.fc[3 * f], y = a.fc[3 * f + 1], z = a.fc[3 * f + 2];
+		a.wall_terms[i] = fy;
+		a.wall_terms[(size_t)a.n_wall + i] = fx;
+		a.wall_terms[2 * (size_t)a.n_wall + i] = y * fz - z * fy;
+		a.wall_terms[3 * (size_t)a.n_wall + i] = z * fx - x * fz;
+		a.wall_terms[4 * (size_t)a.n_wall + i] = x * fy - y * fx;
+	}
+}
+
+// Inter-block halo copies i0, i0+stride, ... into both primitive buffers.
+template <class T>
+__device__ __forceinline__ void halo_range(const FusedView<T>& vf, const PersistArgs& a, int i0, int stride) {
+	for (int i = i0; i < a.n_halo; i += stride) {
+		const Q5<T> q = ld5(vf.Pin, vf.NA, a.halo_src[i]);
+		st5(const_cast<T*>(vf.Pin), vf.NA, a.halo_dst[i], q);
+		st5(vf.Pout, vf.NA, a.halo_dst[i], q);
+	}
+}
+
+// Per-block sums of block b into history slot `slot`: tiles in a fixed tree
+// order, wall faces sequentially in the reference's order.
+template <int TPB>
+__device__ __forceinline__ void block_sums(const PersistArgs& a, int b, int slot, double (*red)[TPB],
+                                           double (*wbuf)[WALL_CHUNK / 4]) {
+	const int w0 = a.block_work[b], w1 = a.block_work[b + 1];
+	double acc[5] = {0., 0., 0., 0., 0.};
+	for (int w = w0 + threadIdx.x; w < w1; w += TPB)
+		for (int q = 0; q < 5; q++) acc[q] += a.wpart[(size_t)w * 5 + q];
+	for (int q = 0; q < 5; q++) red[q][threadIdx.x] = acc[q];
+	__syncthreads();
+	for (int h = TPB / 2; h > 0; h >>= 1) {
+		if (threadIdx.x < h)
+			for (int q = 0; q < 5; q++) red[q][threadIdx.x] += red[q][threadIdx.x + h];
+		__syncthreads();
+	}
+	double* out = a.hist + (size_t)slot * a.stride + b * 10;
+	if (threadIdx.x < 5) {
+		out[threadIdx.x] = red[threadIdx.x][0];
+		if (!isfinite(red[threadIdx.x][0]) && w1 > w0) *a.d_bad = 1;
+	}
+	const int beg = a.wall_off[b], end = a.wall_off[b + 1];
+	double fs = 0.;
+	constexpr int CH = WALL_CHUNK / 4;
+	for (int base_i = beg; base_i < end; base_i += CH) {
+		const int n = min(CH, end - base_i);
+		__syncthreads();
+		for (int j = threadIdx.x; j < 5 * n; j += TPB) {
+			const int q = j / n, i = j - q * n;
+			wbuf[q][i] = a.wall_terms[(size_t)q * a.n_wall + base_i + i];
+		}
+		__syncthreads();
+		if (threadIdx.x < 5)
+			for (int i = 0; i < n; i++) fs += wbuf[threadIdx.x][i];
+	}
+	if (threadIdx.x < 5) out[5 + threadIdx.x] = fs;
+	__syncthreads();
+}
+
+// Persistent form: one cooperative launch runs `iters` outer iterations;
+// phases are separated by grid-wide barriers.  Tiles of converged cases are
+// absent from the work list.
 template <class T, int GRAD, int LIM, int SCHEME, bool ORDER2, int TPB>
 __global__ void __launch_bounds__(TPB, 512 / TPB) k_persistent(FusedView<T> v0, FusedView<T> v1, Physics ph,
                                                                PersistArgs a) {
@@ -828,87 +917,64 @@ __global__ void __launch_bounds__(TPB, 512 / TPB) k_persistent(FusedView<T> v0, 
 			parity ^= 1;
 		}
 		const FusedView<T>& vf = parity ? v1 : v0;  // Pin of the next stage = current state
-		// per-tile residual sums (fixed tree order)
-		for (int w = blockIdx.x; w < a.n_work; w += gridDim.x) {
-			const int4 t = a.work[w];
-			double acc[5] = {0., 0., 0., 0., 0.};
-			for (int c = t.x + threadIdx.x; c < t.y; c += TPB)
-				for (int q = 0; q < 5; q++) {
-					const double r = (double)vf.Rc[q * vf.NR + c] - (double)vf.Rd[q * vf.NR + c];
-					acc[q] += r * r;
-				}
-			for (int q = 0; q < 5; q++) red[q][threadIdx.x] = acc[q];
-			__syncthreads();
-			for (int h = TPB / 2; h > 0; h >>= 1) {
-				if (threadIdx.x < h)
-					for (int q = 0; q < 5; q++) red[q][threadIdx.x] += red[q][threadIdx.x + h];
-				__syncthreads();
-			}
-			if (threadIdx.x < 5) a.wpart[(size_t)w * 5 + threadIdx.x] = red[threadIdx.x][0];
-			__syncthreads();
-		}
-		// wall terms of every wall face (frozen cases included: cheap, ignored by the host)
-		for (int i = blockIdx.x * TPB + threadIdx.x; i < a.n_wall; i += gridDim.x * TPB) {
-			const int f = a.wall_face[i];
-			const double p0 = (double)vf.Pin[4 * (size_t)vf.NA + a.face_lr[2 * f]];
-			const double p1 = (double)vf.Pin[4 * (size_t)vf.NA + a.face_lr[2 * f + 1]];
-			const double cp = (0.5 * (p0 + p1) - 1.) / (a.wall_denom ? a.wall_denom[i] : a.denom);
-			const double fx = cp * a.S[3 * f], fy = cp * a.S[3 * f + 1], fz = cp * a.S[3 * f + 2];
-			const double x = a.fc[3 * f], y = a.fc[3 * f + 1], z = a.fc[3 * f + 2];
-			a.wall_terms[i] = fy;
-			a.wall_terms[(size_t)a.n_wall + i] = fx;
-			a.wall_terms[2 * (size_t)a.n_wall + i] = y * fz - z * fy;
-			a.wall_terms[3 * (size_t)a.n_wall + i] = z * fx - x * fz;
-			a.wall_terms[4 * (size_t)a.n_wall + i] = x * fy - y * fx;
-		}
-		// inter-block halo into both primitive buffers
-		for (int i = blockIdx.x * TPB + threadIdx.x; i < a.n_halo; i += gridDim.x * TPB) {
-			const Q5<T> q = ld5(vf.Pin, vf.NA, a.halo_src[i]);
-			st5(const_cast<T*>(vf.Pin), vf.NA, a.halo_dst[i], q);
-			st5(vf.Pout, vf.NA, a.halo_dst[i], q);
-		}
+		for (int w = blockIdx.x; w < a.n_work; w += gridDim.x) tile_norms<T, TPB>(vf, a, w, red);
+		wall_terms_range(vf, a, blockIdx.x * TPB + threadIdx.x, gridDim.x * TPB);
+		halo_range(vf, a, blockIdx.x * TPB + threadIdx.x, gridDim.x * TPB);
 		grid.sync();
-		// per-block sums into the history: tiles in a fixed tree order, wall
-		// faces sequentially in the reference's order
 		const int slot = min(base + it, a.hist_capacity - 1);
-		for (int b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
-			const int w0 = a.block_work[b], w1 = a.block_work[b + 1];
-			double acc[5] = {0., 0., 0., 0., 0.};
-			for (int w = w0 + threadIdx.x; w < w1; w += TPB)
-				for (int q = 0; q < 5; q++) acc[q] += a.wpart[(size_t)w * 5 + q];
-			for (int q = 0; q < 5; q++) red[q][threadIdx.x] = acc[q];
-			__syncthreads();
-			for (int h = TPB / 2; h > 0; h >>= 1) {
-				if (threadIdx.x < h)
-					for (int q = 0; q < 5; q++) red[q][threadIdx.x] += red[q][threadIdx.x + h];
-				__syncthreads();
-			}
-			double* out = a.hist + (size_t)slot * a.stride + b * 10;
-			if (threadIdx.x < 5) {
-				out[threadIdx.x] = red[threadIdx.x][0];
-				if (!isfinite(red[threadIdx.x][0]) && w1 > w0) *a.d_bad = 1;
-			}
-			const int beg = a.wall_off[b], end = a.wall_off[b + 1];
-			double fs = 0.;
-			constexpr int CH = WALL_CHUNK / 4;
-			for (int base_i = beg; base_i < end; base_i += CH) {
-				const int n = min(CH, end - base_i);
-				__syncthreads();
-				for (int j = threadIdx.x; j < 5 * n; j += TPB) {
-					const int q = j / n, i = j - q * n;
-					wbuf[q][i] = a.wall_terms[(size_t)q * a.n_wall + base_i + i];
-				}
-				__syncthreads();
-				if (threadIdx.x < 5)
-					for (int i = 0; i < n; i++) fs += wbuf[threadIdx.x][i];
-			}
-			if (threadIdx.x < 5) out[5 + threadIdx.x] = fs;
-			__syncthreads();
-		}
+		for (int b = blockIdx.x; b < a.nblocks; b += gridDim.x) block_sums<TPB>(a, b, slot, red, wbuf);
 		grid.sync();
 	}
 	if (blockIdx.x == 0 && threadIdx.x == 0) *a.d_iter = base + a.iters;
 }
+
+// Tiled per-pass form: the same phases as separate launches over the work
+// list (one block of 128 threads per tile of at most 128 cells), captured in a
+// CUDA graph by the host.  Each pass keeps only its own registers and shared
+// memory, so more warps stay resident than in the persistent kernel.
+template <class T, int GRAD, int LIM, bool FIRST>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_recon_tiles(FusedView<T> v, Physics ph, int carry_w0,
+                                                                             const int4* __restrict__ work) {
+	const int4 t = work[blockIdx.x];
+	const int c = t.x + threadIdx.x;
+	if (c < t.y) recon_cell<T, GRAD, LIM, FIRST, 4>(v, ph, carry_w0, c);
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_start_tiles(FusedView<T> v, Physics ph, int carry_w0,
+                                                     const int4* __restrict__ work) {
+	const int4 t = work[blockIdx.x];
+	const int c = t.x + threadIdx.x;
+	if (c < t.y) start_cell<T, 4>(v, ph, carry_w0, c);
+}
+
+template <class T, int SCHEME, bool ORDER1, bool DISS>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update_tiles(FusedView<T> v, Physics ph, T alpha,
+                                                                                   T beta, int last, int carry_w0,
+                                                                                   const int4* __restrict__ work) {
+	const int4 t = work[blockIdx.x];
+	const int c = t.x + threadIdx.x;
+	if (c < t.y) flux_update_cell<T, SCHEME, ORDER1, 4, DISS>(v, ph, alpha, beta, last, carry_w0, c);
+}
+
+// end of an iteration, part 1 (grid = n_work): tile norms, wall terms, halo
+template <class T>
+__global__ void __launch_bounds__(128) k_iter_tail(FusedView<T> vf, PersistArgs a) {
+	__shared__ double red[5][128];
+	tile_norms<T, 128>(vf, a, blockIdx.x, red);
+	wall_terms_range(vf, a, blockIdx.x * 128 + threadIdx.x, gridDim.x * 128);
+	halo_range(vf, a, blockIdx.x * 128 + threadIdx.x, gridDim.x * 128);
+}
+
+// end of an iteration, part 2 (grid = nblocks): per-block sums into history slot *d_iter + it
+__global__ void __launch_bounds__(128) k_iter_sums(PersistArgs a, int it) {
+	__shared__ double red[5][128];
+	__shared__ double wbuf[5][WALL_CHUNK / 4];
+	const int slot = min(*a.d_iter + it, a.hist_capacity - 1);
+	block_sums<128>(a, blockIdx.x, slot, red, wbuf);
+}
+
+__global__ void k_iter_add(int* d_iter, int n) { *d_iter += n; }
 
 }  // namespace
 }  // namespace e3d

@@ -63,6 +63,10 @@ int persistent_blocks_per_sm(int grad, int lim, int scheme, bool order2);
 template <class T>
 cudaError_t launch_persistent(const FusedView<T>& v0, const FusedView<T>& v1, const Physics& ph, const PersistArgs& a,
                               int grad, int lim, int scheme, bool order2, int grid, cudaStream_t st);
+// the same iterations as separate per-pass launches over the work list
+template <class T>
+cudaError_t launch_tiled_iterations(const FusedView<T>& v0, const FusedView<T>& v1, const Physics& ph,
+                                    const PersistArgs& a, int grad, int lim, int scheme, bool order2, cudaStream_t st);
 
 template <class T>
 void launch_flux_update(const FusedView<T>&, const Physics&, int scheme, bool order1, double alpha, double beta,

@@ -1,0 +1,149 @@
+"""Mach/alpha polar sweeps: seeded case lists, the plain per-case solve, and the
+batched + learned solve (every case in one batch, surrogate warm start, FP32
+until the FP32 rounding floor, then FP64 to the target drop).
+
+The reference runs one case per process (Solver/src/Solver.cpp:76-97 loops a
+single mesh until PostProcessing.cpp:77 finds ro_convergence_ <= criterion);
+a sweep there is many such runs.  The plain arm here is that same loop on the
+GPU, case after case, through the FP64 drop-in path.  The batched arm solves
+the same discrete equations: per case it stops at the same density drop,
+measured from the same reference residual (the freestream start's first
+iteration), so both reach the same converged Cl/Cd.
+"""
+from __future__ import annotations
+
+import multiprocessing as mp
+import os
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import api
+from . import meshgen as mg
+
+
+@dataclass
+class CaseSpec:
+    name: str
+    n: int           # hexahedra per side (6 n^3 tetrahedra)
+    mach: float
+    aoa_deg: float
+
+
+def polar_specs(seed: int, count: int, n_range=(25, 60), mach_range=(0.3, 0.8), aoa_range=(-2.0, 6.0),
+                prefix="case") -> list[CaseSpec]:
+    """Seeded sweep: n ~ U{n_range}, Mach ~ U[mach_range], alpha ~ U[aoa_range] (numpy PCG64)."""
+    rng = np.random.default_rng(seed)
+    n = rng.integers(n_range[0], n_range[1] + 1, count)
+    mach = rng.uniform(mach_range[0], mach_range[1], count)
+    aoa = rng.uniform(aoa_range[0], aoa_range[1], count)
+    return [CaseSpec(f"{prefix}{seed}_{i}", int(n[i]), float(mach[i]), float(aoa[i])) for i in range(count)]
+
+
+def _write_one(args):
+    directory, spec, scheme, sides = args
+    d = mg.Deck(topology="", mach=spec.mach, aoa_deg=spec.aoa_deg, max_iter=1000000, criterion=-15.0, **scheme)
+    return mg.write_case(os.path.join(directory, spec.name), spec.n, 1, prefix=spec.name, deck=d, sides=sides)
+
+
+def write_cases(directory: str, specs: list[CaseSpec], scheme: dict, sides: str = "farfield",
+                processes: int | None = None) -> list[str]:
+    """Write every case (SU2 block, .top, deck) in parallel; returns the deck paths in spec order.
+
+    Worker processes are started with 'spawn', so this is safe after CUDA has
+    been initialised in the calling process."""
+    jobs = [(directory, s, scheme, sides) for s in specs]
+    procs = processes or min(len(jobs), os.cpu_count() or 1, 32)
+    if procs <= 1:
+        return [_write_one(j) for j in jobs]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(_write_one, jobs, chunksize=1)
+
+
+def _first_below(conv: np.ndarray, level: float) -> int | None:
+    hit = np.nonzero(conv <= level)[0]
+    return int(hit[0]) + 1 if hit.size else None
+
+
+def solve_plain(case: api.Case, criterion: float, max_iter: int, check_every: int = 50,
+                precision: str = "fp64") -> dict:
+    """The reference's loop on the GPU for one case: freestream start, fused
+    iterations until the density drop reaches `criterion`."""
+    s = api.Solver(case, precision=precision, hist_capacity=max(4096, check_every * 4))
+    t0 = time.perf_counter()
+    s.solve(max_iter, criterion, check_every)
+    wall = time.perf_counter() - t0
+    h = s.history()
+    c = h["conv"][:, 0]
+    out = dict(iters=len(c), reached=_first_below(c, criterion), wall_s=wall, cl=float(h["cl"][-1]),
+               cd=float(h["cd"][-1]), cells=sum(case.block_info(b).n_real for b in range(case.n_blocks)))
+    s.close()
+    return out
+
+
+def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrogate: api.Surrogate | None = None,
+                  switch_at: float | None = -4.0, iters_per_launch: int = 50, stall_window: int = 3000) -> dict:
+    """All cases in one batch: one freestream iteration (the reference residual
+    of each case's drop), the surrogate's warm start when given, FP32
+    iterations to `switch_at` (a case stalled for `stall_window` iterations
+    also moves on), then FP64 iterations to `criterion`; each case leaves the
+    work list once it gets there."""
+    t0 = time.perf_counter()
+    b = api.Batch(cases, precision="fp32" if switch_at is not None else "fp64",
+                  hist_capacity=max(4096, iters_per_launch * 4))
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b.solve_batch(1, -1e300, iters_per_launch=1)
+    fallback = 0
+    t_warm = 0.0
+    if surrogate is not None:
+        tw = time.perf_counter()
+        fallback = surrogate.warm_start(b)
+        t_warm = time.perf_counter() - tw
+    phases = []
+    if switch_at is not None:
+        tp = time.perf_counter()
+        b.solve_batch(max_iter, switch_at, iters_per_launch=iters_per_launch, stall_window=stall_window)
+        phases.append(dict(precision="fp32", to=switch_at, wall_s=time.perf_counter() - tp, tuning=b.tuning()))
+        tp = time.perf_counter()
+        api.set_precision(b, "fp64")
+        phases.append(dict(precision="switch", wall_s=time.perf_counter() - tp))
+    tp = time.perf_counter()
+    b.solve_batch(max_iter, criterion, iters_per_launch=iters_per_launch)
+    phases.append(dict(precision="fp64", to=criterion, wall_s=time.perf_counter() - tp, tuning=b.tuning()))
+    wall = time.perf_counter() - t0
+    per_case = []
+    for c in range(len(cases)):
+        h = b.case_history(c)
+        cv = h["conv"][:, 0]
+        per_case.append(dict(iters=len(cv), reached=_first_below(cv, criterion), cl=float(h["cl"][-1]),
+                             cd=float(h["cd"][-1])))
+    b.close()
+    return dict(wall_s=wall, setup_s=t_setup, warm_s=t_warm, fallback=fallback, phases=phases, cases=per_case)
+
+
+def train_surrogate(cases: list[api.Case], seed: int, criterion: float = -4.0, max_iter: int = 200000,
+                    steps: int = 6000, batch: int = 16384, lr: float = 3e-3, iters_per_launch: int = 200,
+                    group: int = 64, stall_window: int = 3000) -> tuple[api.Surrogate, dict]:
+    """Solves the training cases in batches of `group` (FP32, freestream start)
+    to `criterion`, adds every real cell's converged state to the surrogate's
+    sample store, and trains it."""
+    m = api.Surrogate(seed=seed, gamma=1.4)
+    t0 = time.perf_counter()
+    cell_iters = 0
+    for g0 in range(0, len(cases), group):
+        part = cases[g0:g0 + group]
+        b = api.Batch(part, precision="fp32", hist_capacity=max(4096, iters_per_launch * 4))
+        b.solve_batch(max_iter, criterion, iters_per_launch=iters_per_launch, stall_window=stall_window)
+        for c, case in enumerate(part):
+            cell_iters += int(b.case_history(c)["conv"].shape[0]) * sum(
+                case.block_info(k).n_real for k in range(case.n_blocks))
+        m.add_solution(b)
+        b.close()
+    t_solve = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss, hist = m.train(steps, batch=batch, lr=lr)
+    t_train = time.perf_counter() - t0
+    return m, dict(samples=m.n_samples, solve_s=t_solve, train_s=t_train, loss=loss,
+                   loss_first=float(np.mean(hist[:20])), cell_iters=cell_iters)

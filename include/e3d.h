@@ -156,15 +156,20 @@ int e3d_state_set(e3d_solver* s, int block, const char* name, const double* src,
  * and chord.  e3d_batch_solve advances all cases together with the persistent
  * cooperative kernel (FP32 variant, tetrahedral meshes): one graph-captured
  * launch runs `iters_per_launch` outer iterations over a work list of tiles;
- * a case leaves the work list once its density drop reaches `criterion` or it
- * has run max_iter iterations.  The first call autotunes the tile size and
- * the grid (cached per problem-size bucket, and in $E3D_AUTOTUNE_CACHE if set).
+ * a case leaves the work list once its density drop reaches `criterion`, it
+ * has run max_iter iterations in all, or (stall_window > 0) its last
+ * stall_window iterations brought no new minimum 0.05 decades below the
+ * earlier ones.  The first call autotunes the tile size and
+ * the form: the persistent cooperative kernel with a tuned grid, or the same
+ * phases as separate per-pass launches over the tiles in one captured graph
+ * (cached per problem-size bucket, and in $E3D_AUTOTUNE_CACHE if set;
+ * e3d_batch_tuning reports *grid = 0 for the per-pass form).
  * iters_done[c] = iterations case c needed (n_cases entries);
  * *device_ms = device time of the whole solve.  e3d_iterate also works on a
  * batch (every case advances; no per-case stop). */
 int e3d_batch_create(const e3d_case* const* cases, int n_cases, const e3d_options* opt, e3d_solver** out);
-int e3d_batch_solve(e3d_solver* s, int max_iter, double criterion, int iters_per_launch, int* iters_done,
-                    double* device_ms);
+int e3d_batch_solve(e3d_solver* s, int max_iter, double criterion, int iters_per_launch, int stall_window,
+                    int* iters_done, double* device_ms);
 int e3d_case_count(const e3d_solver* s, int* n);
 int e3d_case_history_length(const e3d_solver* s, int case_index, int* n);
 int e3d_case_history(const e3d_solver* s, int case_index, int first, int count, e3d_iter_record* out);

@@ -65,23 +65,27 @@ def test_batch_graph_path_matches_single_cases_fp64(tmp_path, opts):
         fb += case.n_blocks
 
 
+@pytest.mark.parametrize("form", ["persistent", "per-pass"])
 @pytest.mark.parametrize("opts", [O2_AUSM, O2_ROE, O1_ROE], ids=["o2_gg_bj_ausm", "o2_ls_venk_roe", "o1_roe"])
-def test_batch_persistent_matches_single_cases_fp64(tmp_path, opts):
+def test_batch_persistent_matches_single_cases_fp64(tmp_path, monkeypatch, opts, form):
+    monkeypatch.setenv("E3D_BATCH_FORM", form)
     cases = _cases(tmp_path, opts)
     batch = api.Batch(cases, precision="fp64")
     done, ms = batch.solve_batch(12, NEVER, iters_per_launch=5)
     assert list(done) == [12] * len(cases) and ms > 0
     t = batch.tuning()
-    assert t["tile_cells"] in (128, 256, 512) and t["grid"] > 0
+    assert t["tile_cells"] in (128, 256, 512) and t["mode"] == form
     fb = 0
     for c, case in enumerate(cases):
         _check_case(batch, c, fb, _single(case, "fp64", 12))
         fb += case.n_blocks
 
 
-def test_batch_freezes_converged_cases_fp64(tmp_path):
+@pytest.mark.parametrize("form", ["persistent", "per-pass"])
+def test_batch_freezes_converged_cases_fp64(tmp_path, monkeypatch, form):
     """A case leaves the work list after the launch in which it reached the
     criterion; its state is then the single-case state of that many iterations."""
+    monkeypatch.setenv("E3D_BATCH_FORM", form)
     cases = _cases(tmp_path, O1_ROE)
     K, ipl = 40, 4
     singles = [_single(c, "fp64", K) for c in cases]
@@ -103,7 +107,9 @@ def test_batch_freezes_converged_cases_fp64(tmp_path):
         fb += case.n_blocks
 
 
-def test_batch_fp32_persistent_tracks_fp32_graph(tmp_path):
+@pytest.mark.parametrize("form", ["persistent", "per-pass"])
+def test_batch_fp32_persistent_tracks_fp32_graph(tmp_path, monkeypatch, form):
+    monkeypatch.setenv("E3D_BATCH_FORM", form)
     cases = _cases(tmp_path, O2_AUSM)
     a = api.Batch(cases, precision="fp32")
     a.solve_batch(20, NEVER, iters_per_launch=10)
