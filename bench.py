@@ -324,7 +324,7 @@ def run_sweep_workload(a, rank, world):
             train, test = cases[:len(tr_specs)], cases[len(tr_specs):]
             log(f"[bench] {len(cases)} cases written and loaded in {time.time() - t0:.1f}s")
             crit, max_iter = -8.0, 200000
-            m, tinfo = sw.train_surrogate(train, seed=1000, criterion=-4.0, steps=6000 if not small else 3000)
+            m, tinfo = sw.train_surrogate(train, seed=1000, criterion=-4.0, steps=40000 if not small else 5000)
             log(f"[bench] surrogate: {tinfo}")
             clocks.mark("start")
             learned = sw.solve_batched(test, crit, max_iter, surrogate=m)

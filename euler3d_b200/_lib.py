@@ -21,7 +21,7 @@ ERRORS = {
 GRAD = {"greengauss": 0, "leastsquares": 1}
 LIM = {"barthjespersen": 0, "venkatakrishnan": 1}
 FLUX = {"roe": 0, "ausm": 1}
-FP64, FP32 = 0, 1
+FP64, FP32, FP64_FMA = 0, 1, 2
 SURROGATE_PARAMS, SURROGATE_NORM = 36232, 24
 
 

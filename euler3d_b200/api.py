@@ -253,9 +253,11 @@ class Batch(Solver):
 
 
 def set_precision(solver: Solver, precision: str) -> None:
-    """Switch an FP32 solver (or batch) to FP64 in place."""
-    L.check(L.lib().e3d_solver_set_precision(solver._h, L.FP64 if precision == "fp64" else L.FP32))
-    solver.precision = precision
+    """Switch an FP32 solver (or batch) to FP64 in place: "fp64", or "fp64-fma" for batch
+    solves with the FP64 kernels built with fused multiply-add."""
+    code = {"fp64": L.FP64, "fp64-fma": L.FP64_FMA, "fp32": L.FP32}[precision]
+    L.check(L.lib().e3d_solver_set_precision(solver._h, code))
+    solver.precision = "fp32" if precision == "fp32" else "fp64"
 
 
 def cell_features(solver: Solver) -> np.ndarray:

@@ -302,9 +302,12 @@ int e3d_batch_tuning(const e3d_solver* s, int* tile_cells, int* grid, double* ms
 
 int e3d_solver_set_precision(e3d_solver* s, int precision) {
 	return guard([&] {
-		if (precision == E3D_FP64) eng(s).widen_to_fp64();
-		else if (eng(s).precision() != e3d::PREC_FP32)
+		if (precision == E3D_FP64 || precision == E3D_FP64_FMA) {
+			eng(s).widen_to_fp64();
+			eng(s).set_fp64_contracted(precision == E3D_FP64_FMA);
+		} else if (precision != E3D_FP32 || eng(s).precision() != e3d::PREC_FP32) {
 			throw e3d::Error(E3D_ERR_ARG, "a solver switches from FP32 to FP64 only");
+		}
 	});
 }
 

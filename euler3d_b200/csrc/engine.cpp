@@ -11,6 +11,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 
 namespace e3d {
 
@@ -1289,9 +1290,14 @@ double Engine::run_persistent_t(int iters) {
 	};
 	const FusedView<T> v0 = view(false), v1 = view(true);
 	const int grid = tiled_ ? n_work_ : std::max(1, std::min(grid_, n_work_));
+	const bool fast = std::is_same<T, double>::value && fast64_;
 	auto launch = [&]() {
-		return tiled_ ? launch_tiled_iterations<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, order_ == 2, st_)
-		              : launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, order_ == 2, grid, st_);
+		const bool o2 = order_ == 2;
+		if (fast)
+			return tiled_ ? batch_fast::launch_tiled_iterations<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, o2, st_)
+			              : batch_fast::launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, o2, grid, st_);
+		return tiled_ ? batch::launch_tiled_iterations<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, o2, st_)
+		              : batch::launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, o2, grid, st_);
 	};
 	cudaEvent_t e0, e1;
 	cuda_ok(cudaEventCreate(&e0), "event");
@@ -1377,12 +1383,13 @@ void Engine::autotune(int iters) {
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	const bool o2 = order_ == 2;
-	const int maxb = opt_.precision == PREC_FP32 ? persistent_blocks_per_sm<float>(grad_kind_, lim_kind_, scheme_, o2)
-	                                             : persistent_blocks_per_sm<double>(grad_kind_, lim_kind_, scheme_, o2);
+	const int maxb = opt_.precision == PREC_FP32 ? batch::persistent_blocks_per_sm<float>(grad_kind_, lim_kind_, scheme_, o2)
+	                 : fast64_ ? batch_fast::persistent_blocks_per_sm<double>(grad_kind_, lim_kind_, scheme_, o2)
+	                           : batch::persistent_blocks_per_sm<double>(grad_kind_, lim_kind_, scheme_, o2);
 	if (maxb <= 0) throw Error(E3D_ERR_CUDA, "persistent kernel cannot be resident");
 	int bucket = 0;
 	while ((1LL << bucket) < (long long)NR_) bucket++;
-	const TuneKey key{bucket, scheme_, grad_kind_, lim_kind_, order_ + 4 * (int)opt_.precision};
+	const TuneKey key{bucket, scheme_, grad_kind_, lim_kind_, order_ + 4 * (int)opt_.precision + 8 * (int)fast64_};
 	// E3D_BATCH_FORM=persistent or per-pass restricts the search (and bypasses the cache)
 	const char* form_env = std::getenv("E3D_BATCH_FORM");
 	const std::string form = form_env ? form_env : "";
@@ -1544,6 +1551,18 @@ int Engine::apply_conservative(const float* dev_w, int ld) {
 	cuda_ok(cudaMemcpyAsync(&n, fallback_d_.p, sizeof(int), cudaMemcpyDeviceToHost, st_), "fallback count");
 	cuda_ok(cudaStreamSynchronize(st_), "sync");
 	return n;
+}
+
+void Engine::set_fp64_contracted(bool on) {
+	if (opt_.precision != PREC_FP64) throw Error(E3D_ERR_STATE, "contracted FP64 batch kernels need an FP64 solver");
+	if (fast64_ == on) return;
+	fast64_ = on;
+	if (pgraph_) {
+		cudaGraphExecDestroy(pgraph_);
+		pgraph_ = nullptr;
+	}
+	grid_ = 0;
+	tuning_ = Tuning{};
 }
 
 void Engine::widen_to_fp64() {

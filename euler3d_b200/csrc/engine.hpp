@@ -112,6 +112,10 @@ public:
 	// FP32 solver -> FP64 solver in place: FP64 geometry and state (real cells from the carried FP64
 	// conservative state), histories and reference norms kept, FP32 buffers released
 	void widen_to_fp64();
+	// FP64 batch solves with the kernels built with fused multiply-add (same discrete equations, last-bit
+	// differences from the bit-identical FP64 path); affects e3d_batch_solve only
+	void set_fp64_contracted(bool on);
+	bool fp64_contracted() const { return fast64_; }
 	long long n_real_case(int c) const;
 	void sync();  // waits for queued work; throws on a CUDA error or a non-finite norm
 
@@ -213,7 +217,7 @@ private:
 	Tuning tuning_;
 	cudaGraphExec_t pgraph_ = nullptr;
 	int pgraph_iters_ = 0, pgraph_parity_ = -1, pgraph_grid_ = 0;
-	bool tiled_ = false, pgraph_tiled_ = false;
+	bool tiled_ = false, pgraph_tiled_ = false, fast64_ = false;
 	void build_work();
 	double run_persistent(int iters);
 	template <class T>

@@ -4,6 +4,7 @@
 #include "kernels.cuh"
 #include "launch.hpp"
 #include "launch_common.cuh"
+#include "batch_launch.cuh"
 
 namespace e3d {
 
@@ -64,11 +65,11 @@ template void launch_recon<double>(const FusedView<double>&, const Physics&, int
 template void launch_start<double>(const FusedView<double>&, const Physics&, int, cudaStream_t);
 template void launch_flux_update<double>(const FusedView<double>&, const Physics&, int, bool, double, double, int, int,
                                          cudaStream_t);
-template int persistent_blocks_per_sm<double>(int, int, int, bool);
-template cudaError_t launch_persistent<double>(const FusedView<double>&, const FusedView<double>&, const Physics&,
+template int batch::persistent_blocks_per_sm<double>(int, int, int, bool);
+template cudaError_t batch::launch_persistent<double>(const FusedView<double>&, const FusedView<double>&, const Physics&,
                                                const PersistArgs&, int, int, int, bool, int, cudaStream_t);
 
-template cudaError_t launch_tiled_iterations<double>(const FusedView<double>&, const FusedView<double>&, const Physics&,
+template cudaError_t batch::launch_tiled_iterations<double>(const FusedView<double>&, const FusedView<double>&, const Physics&,
                                                     const PersistArgs&, int, int, int, bool, cudaStream_t);
 
 }  // namespace e3d

@@ -56,8 +56,13 @@ void launch_recon(const FusedView<T>&, const Physics&, int grad, int lim, bool f
 template <class T>
 void launch_start(const FusedView<T>&, const Physics&, int carry, cudaStream_t);
 
-// persistent batch kernel: threads per block, resident blocks per SM, launch
+// batch launchers: threads per block; per namespace: resident blocks per SM of
+// the persistent kernel, its cooperative launch, and the tiled per-pass form.
+// `batch` is built with the working precision's flags (FP64: no contraction,
+// the same arithmetic as the single-case path); `batch_fast` holds FP64
+// kernels built with FMA contraction (k64f.cu).
 constexpr int kPersistThreads = 128;
+namespace batch {
 template <class T>
 int persistent_blocks_per_sm(int grad, int lim, int scheme, bool order2);
 template <class T>
@@ -67,6 +72,18 @@ cudaError_t launch_persistent(const FusedView<T>& v0, const FusedView<T>& v1, co
 template <class T>
 cudaError_t launch_tiled_iterations(const FusedView<T>& v0, const FusedView<T>& v1, const Physics& ph,
                                     const PersistArgs& a, int grad, int lim, int scheme, bool order2, cudaStream_t st);
+}  // namespace batch
+namespace batch_fast {
+template <class T>
+int persistent_blocks_per_sm(int grad, int lim, int scheme, bool order2);
+template <class T>
+cudaError_t launch_persistent(const FusedView<T>& v0, const FusedView<T>& v1, const Physics& ph, const PersistArgs& a,
+                              int grad, int lim, int scheme, bool order2, int grid, cudaStream_t st);
+// the same iterations as separate per-pass launches over the work list
+template <class T>
+cudaError_t launch_tiled_iterations(const FusedView<T>& v0, const FusedView<T>& v1, const Physics& ph,
+                                    const PersistArgs& a, int grad, int lim, int scheme, bool order2, cudaStream_t st);
+}  // namespace batch_fast
 
 template <class T>
 void launch_flux_update(const FusedView<T>&, const Physics&, int scheme, bool order1, double alpha, double beta,

@@ -83,15 +83,19 @@ def solve_plain(case: api.Case, criterion: float, max_iter: int, check_every: in
 
 
 def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrogate: api.Surrogate | None = None,
-                  switch_at: float | None = -4.0, iters_per_launch: int = 50, stall_window: int = 3000) -> dict:
+                  switch_at: float | None = -4.5, iters_per_launch: int = 50, stall_window: int = 3000,
+                  fp64: str = "fp64-fma") -> dict:
     """All cases in one batch: one freestream iteration (the reference residual
     of each case's drop), the surrogate's warm start when given, FP32
     iterations to `switch_at` (a case stalled for `stall_window` iterations
-    also moves on), then FP64 iterations to `criterion`; each case leaves the
-    work list once it gets there."""
+    also moves on), then FP64 iterations to `criterion` (`fp64`: "fp64-fma"
+    for the kernels built with fused multiply-add, "fp64" for the
+    bit-identical ones); each case leaves the work list once it gets there."""
     t0 = time.perf_counter()
     b = api.Batch(cases, precision="fp32" if switch_at is not None else "fp64",
                   hist_capacity=max(4096, iters_per_launch * 4))
+    if switch_at is None and fp64 == "fp64-fma":
+        api.set_precision(b, fp64)
     t_setup = time.perf_counter() - t0
     t0 = time.perf_counter()
     b.solve_batch(1, -1e300, iters_per_launch=1)
@@ -107,7 +111,7 @@ def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrog
         b.solve_batch(max_iter, switch_at, iters_per_launch=iters_per_launch, stall_window=stall_window)
         phases.append(dict(precision="fp32", to=switch_at, wall_s=time.perf_counter() - tp, tuning=b.tuning()))
         tp = time.perf_counter()
-        api.set_precision(b, "fp64")
+        api.set_precision(b, fp64)
         phases.append(dict(precision="switch", wall_s=time.perf_counter() - tp))
     tp = time.perf_counter()
     b.solve_batch(max_iter, criterion, iters_per_launch=iters_per_launch)
@@ -124,7 +128,7 @@ def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrog
 
 
 def train_surrogate(cases: list[api.Case], seed: int, criterion: float = -4.0, max_iter: int = 200000,
-                    steps: int = 6000, batch: int = 16384, lr: float = 3e-3, iters_per_launch: int = 200,
+                    steps: int = 40000, batch: int = 32768, lr: float = 3e-3, iters_per_launch: int = 200,
                     group: int = 64, stall_window: int = 3000) -> tuple[api.Surrogate, dict]:
     """Solves the training cases in batches of `group` (FP32, freestream start)
     to `criterion`, adds every real cell's converged state to the surrogate's

@@ -43,6 +43,7 @@ extern "C" {
 
 #define E3D_FP64 0 /* drop-in: reference FP64 arithmetic */
 #define E3D_FP32 1 /* FP32 bulk, FP64 conserved state and reductions */
+#define E3D_FP64_FMA 2 /* e3d_solver_set_precision only: FP64, batch solves with fused multiply-add */
 
 typedef struct e3d_case e3d_case;     /* host case: deck + topology + blocks */
 typedef struct e3d_solver e3d_solver; /* device-resident solver over one case */
@@ -178,8 +179,11 @@ int e3d_batch_tuning(const e3d_solver* s, int* tile_cells, int* grid, double* ms
 /* ---- precision switch, warm start and the learned surrogate -------------------
  * No counterpart in the reference.
  * e3d_solver_set_precision: an FP32 solver becomes an FP64 solver in place
- * (E3D_FP64 only); real cells take the carried FP64 conservative state,
- * histories and the iteration-0 reference norms carry on.  The FP32 path's
+ * (E3D_FP64 or E3D_FP64_FMA); real cells take the carried FP64 conservative
+ * state, histories and the iteration-0 reference norms carry on.  With
+ * E3D_FP64_FMA, e3d_batch_solve runs FP64 kernels built with fused
+ * multiply-add: the same discrete equations and converged solution, not
+ * bit-identical to the reference (E3D_FP64 switches an FP64 solver back).  The FP32 path's
  * residual stops dropping near 5 orders (FP32 rounding of the fluxes); a run
  * to a deeper drop continues in FP64 from there.
  * e3d_cell_features: surrogate inputs of every real cell of every case, in

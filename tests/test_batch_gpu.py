@@ -123,6 +123,31 @@ def test_batch_fp32_persistent_tracks_fp32_graph(tmp_path, monkeypatch, form):
         assert abs(ha["cl"][-1] - hb["cl"][-1]) < 1e-5 * max(1.0, abs(hb["cl"][-1]))
 
 
+@pytest.mark.parametrize("form", ["persistent", "per-pass"])
+def test_batch_fp64_fma_tracks_the_bitwise_batch(tmp_path, monkeypatch, form):
+    """The FP64 batch kernels built with fused multiply-add solve the same
+    equations: after 12 second-order iterations every state within 1e-9.
+    Channel cases: a farfield face the flow runs along switches branch on the
+    sign of u.n, which last-bit differences may flip."""
+    monkeypatch.setenv("E3D_BATCH_FORM", form)
+    cases = []
+    for i, (n, nb, mach, aoa) in enumerate(SWEEP):
+        d = mg.Deck(topology="", mach=mach, aoa_deg=aoa, **O2_ROE)
+        cases.append(api.Case(mg.write_case(str(tmp_path / f"k{i}"), n, nb, prefix=f"k{i}", deck=d,
+                                            sides="channel")))
+    a = api.Batch(cases, precision="fp64")
+    a.solve_batch(12, NEVER, iters_per_launch=6)
+    b = api.Batch(cases, precision="fp64")
+    api.set_precision(b, "fp64-fma")
+    b.solve_batch(12, NEVER, iters_per_launch=6)
+    assert b.tuning()["mode"] == form
+    for blk in range(a.n_blocks):
+        pa, pb = a.get(blk, "prim"), b.get(blk, "prim")
+        assert max_rel(pb, pa, floor=1e-3) < 1e-9
+    for c in range(len(cases)):
+        assert abs(a.case_history(c)["cl"][-1] - b.case_history(c)["cl"][-1]) < 1e-9
+
+
 def test_batch_fp32_against_fp64_single(tmp_path):
     """FP32 batch within the FP32 variant's bar of each FP64 single case."""
     cases = _cases(tmp_path, O1_ROE, sweep=SWEEP[:2])
