@@ -54,6 +54,34 @@ def make_case(directory: str, n: int, blocks: int) -> str:
     return mg.write_case(directory, n, blocks, deck=deck)
 
 
+WING_SCHEME = dict(order=2, flux="ausm", gradient="leastsquares", limiter="barthjespersen", omega=2.16e-16, k=5.0,
+                   mach=0.8, aoa_deg=3.0, cfl=1.5, stages=5)
+WING_POINTS = 3_800_000
+
+
+def wing_case(a, td):
+    """The swept-wing case: an existing directory (--mesh-dir) or a fresh one."""
+    from euler3d_b200 import meshgen as mg
+    from euler3d_b200 import wingmesh as wm
+
+    if a.mesh_dir and os.path.exists(os.path.join(a.mesh_dir, "wing.deck")):
+        case_dir = a.mesh_dir
+    else:
+        case_dir = a.mesh_dir or os.path.join(td, "wing")
+        deck = mg.Deck(topology="", max_iter=1000000, criterion=-15.0, **WING_SCHEME)
+        wm.write_wing_case(case_dir, WING_POINTS, n_blocks=16, seed=5, deck=deck)
+    w = WING_SCHEME
+    cfg = {"workload": f"swept trapezoidal wing (NACA 4-digit 12 %, 30 deg sweep, taper 0.56) in a farfield box, "
+                       f"seeded Delaunay tetrahedra (seed 5, {WING_POINTS:,} points requested), 16 x-slab blocks on "
+                       f"one GPU, Morton-ordered cells; {w['gradient']} + {w['limiter']} + {w['flux']}, "
+                       f"M {w['mach']}, alpha {w['aoa_deg']}, {w['stages']}-stage RK, CFL {w['cfl']}",
+           "blocks": 16,
+           "arithmetic": "fp32 fluxes/gradients/limiters, fp64 conserved state and reductions"
+           if a.precision == "fp32" else "fp64 throughout (reference arithmetic)",
+           "l2": "working set (many GB) far larger than the 126 MB L2; no flush needed"}
+    return os.path.join(case_dir, "wing.deck"), case_dir, cfg
+
+
 def workload_config(n, blocks, precision):
     w = WORKLOAD
     return {"workload": f"bump channel {n}^3 hex x 6 tets ({6 * n ** 3:,} tets), {blocks} slab blocks on one GPU, "
@@ -371,9 +399,13 @@ def main():
     ap.add_argument("--blocks", type=int, default=WORKLOAD["blocks"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["channel", "polar", "warmstart"], default="channel",
+    ap.add_argument("--workload", choices=["channel", "polar", "warmstart", "wing"], default="channel",
                     help="channel: the 3.07M-tet second-order case (default); polar: 64-case batched sweep "
-                         "throughput; warmstart: time to an 8-order drop, batched + learned vs plain")
+                         "throughput; warmstart: time to an 8-order drop, batched + learned vs plain; wing: the "
+                         "~20M-tet Delaunay swept wing")
+    ap.add_argument("--mesh-dir", default=None,
+                    help="wing: a directory holding wing.deck (written by euler3d_b200.wingmesh); generated "
+                         "into a temporary directory when absent")
     ap.add_argument("--scale", choices=["full", "small"], default="full",
                     help="small: the same sweep workloads on 10^3..16^3 meshes (quick checks)")
     a = ap.parse_args()
@@ -382,7 +414,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return run_reference_arm(a, rank)
-    if a.workload != "channel":
+    if a.workload not in ("channel", "wing"):
         return run_sweep_workload(a, rank, world)
 
     import torch
@@ -400,7 +432,11 @@ def main():
     steps = max(1, a.steps)
     with tempfile.TemporaryDirectory() as td:
         t0 = time.time()
-        deck = make_case(td, a.n, a.blocks)
+        if a.workload == "wing":
+            deck, case_dir, cfg = wing_case(a, td)
+        else:
+            deck, case_dir = make_case(td, a.n, a.blocks), td
+            cfg = workload_config(a.n, a.blocks, a.precision)
         t1 = time.time()
         case = Case(deck)
         t2 = time.time()
@@ -409,6 +445,7 @@ def main():
         log(f"[bench] rank {rank}: mesh gen {t1 - t0:.1f}s, case load {t2 - t1:.1f}s, solver setup {t3 - t2:.1f}s, "
             f"device bytes {s.device_bytes() / 1e9:.2f} GB")
         cells = sum(case.block_info(b).n_real for b in range(case.n_blocks))
+        cfg["cells"] = cells
         clocks = ClockSampler(local)
         s.iterate(warm)
         s.sync()
@@ -439,7 +476,7 @@ def main():
         traffic = None
         try:
             tr = json.load(open(os.path.join(HERE, "profiles", "ncu_traffic.json")))
-            traffic = tr.get(f"{a.precision}:{dom['name']}")
+            traffic = tr.get(f"{a.precision}:{dom['name']}") if a.workload == "channel" else None
         except Exception:
             pass
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -486,14 +523,14 @@ def main():
         cpu = None
         if rank == 0 and world == 1 and not a.no_cpu_baseline:
             try:
-                cpu = cpu_baseline_single(deck, td)
+                cpu = cpu_baseline_single(deck, case_dir)
             except Exception as e:  # reported, not fatal: the GPU number stands
                 cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
             "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic",
-            "config": dict(workload_config(a.n, a.blocks, a.precision), parallelism=f"replicas{world}"),
+            "config": dict(cfg, parallelism=f"replicas{world}"),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": cl,
             "final": {"iterations": int(len(hist["iter"])), "ro_conv": float(hist["conv"][-1, 0]),
