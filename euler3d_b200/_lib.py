@@ -81,6 +81,7 @@ SIGNATURES = {
     "e3d_flux_diss": ([C.c_void_p, C.c_int, C.c_int, C.c_double], C.c_int),
     "e3d_update_internal": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
     "e3d_update_boundary": ([C.c_void_p, C.c_int], C.c_int),
+    "e3d_smooth_residual": ([C.c_void_p, C.c_int], C.c_int),
     "e3d_halo": ([C.c_void_p], C.c_int),
     "e3d_flow_data": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "e3d_iterate": ([C.c_void_p, C.c_int], C.c_int),

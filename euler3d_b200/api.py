@@ -453,6 +453,13 @@ class NoSmoother:
         return None
 
 
+class CentralIrsSmoother:
+    """CentralIrsSmoother.cpp:12-166: one Jacobi step of central implicit residual smoothing."""
+
+    def smoothResidual(self, block: Block) -> None:
+        L.check(L.lib().e3d_smooth_residual(block.solver._h, block.block_id_))
+
+
 RK_TABLES = {  # Solver/src/RungeKutta.cpp:23-68
     1: ([1.0], [1.0]),
     2: ([0.6, 1.0], [1.0, 0.0]),
@@ -477,9 +484,7 @@ class ResidualCalculator:
             self.flux_scheme_ = AusmScheme(gamma)
         else:
             raise ValueError(f"unknown flux scheme {flux_scheme_choice!r} (roe|ausm)")
-        if residual_smoother_choice:
-            raise ValueError("implicit residual smoothing is not provided by this path")
-        self.residual_smoother_ = NoSmoother()
+        self.residual_smoother_ = CentralIrsSmoother() if residual_smoother_choice else NoSmoother()
 
     def computeResidual(self, block: Block) -> None:
         self.interpolation_.computeInterpolation(block)

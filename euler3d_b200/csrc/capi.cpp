@@ -459,6 +459,7 @@ int e3d_update_internal(e3d_solver* s, int block, double alpha) {
 	return guard([&] { eng(s).update_internal(block, alpha); });
 }
 int e3d_update_boundary(e3d_solver* s, int block) { return guard([&] { eng(s).update_boundary(block); }); }
+int e3d_smooth_residual(e3d_solver* s, int block) { return guard([&] { eng(s).smooth_residual(block); }); }
 int e3d_halo(e3d_solver* s) { return guard([&] { eng(s).halo(); }); }
 
 int e3d_flow_data(e3d_solver* s, double* out, int64_t count) {

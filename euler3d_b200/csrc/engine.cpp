@@ -91,8 +91,8 @@ Engine::Engine(const std::vector<const HostCase*>& cases, const EngineOptions& o
 	order_ = deck_.order == 2 ? 2 : 1;
 	grad_kind_ = deck_.gradient == "leastsquares" ? GRAD_LEAST_SQUARES : GRAD_GREEN_GAUSS;
 	lim_kind_ = deck_.limiter == "venkatakrishnan" ? LIM_VENKATAKRISHNAN : LIM_BARTH_JESPERSEN;
-	if (deck_.smoothing)
-		throw Error(E3D_ERR_ARG, "implicit residual smoothing (deck smoothing = 1) is not provided by this path");
+	if (deck_.smoothing && opt_.precision != PREC_FP64)
+		throw Error(E3D_ERR_ARG, "residual smoothing (deck smoothing = 1) runs on the FP64 path");
 	rk_tables(deck_.stages, alpha_, beta_);
 	// physics constants, computed with the reference's expressions on the host
 	ph_.gamma = deck_.gamma;
@@ -414,6 +414,7 @@ void Engine::init_state() {
 		f32_.FS.alloc(order_ == 2 ? 5 * (size_t)NS_ : 0);
 	}
 	W0_.upload(zR);
+	if (deck_.smoothing) irs_.alloc(10 * (size_t)NR_);  // before any graph capture
 	if (carry_) {
 		// W carried in FP64 from the freestream conservative state
 		std::vector<double> W(5 * (size_t)NR_);
@@ -572,6 +573,14 @@ void Engine::update_internal(int block, double alpha) {
 	launch_update(E3D_GEO, state64(), ph_, alpha, r0, r1, st_);
 	check("update_internal");
 }
+void Engine::smooth_residual(int block) {
+	require_fp64("smooth_residual");
+	int r0, r1, g0, g1;
+	block_range(block, r0, r1, g0, g1);
+	if (irs_.n < 10 * (size_t)NR_) irs_.alloc(10 * (size_t)NR_);
+	launch_smooth(E3D_GEO, state64(), irs_.p, r0, r1, st_);
+	check("smooth_residual");
+}
 void Engine::update_boundary(int block) {
 	require_fp64("update_boundary");
 	int r0, r1, g0, g1;
@@ -636,8 +645,42 @@ void Engine::flow_data(std::vector<double>& out) {
 // One outer iteration (Solver::solve body, Solver.cpp:83-96, all blocks at
 // once): W0 + time step, the RK stages (RungeKutta.cpp:85-92), norms and forces
 // (PostProcessing::computeFlowData), then the inter-block halo.
+// One outer iteration with residual smoothing (deck smoothing = 1): the
+// reference's call sequence on the FP64 strategy-level kernels
+// (RungeKutta.cpp:85-92, ResidualCalculator.cpp:24-41 with the smoother between
+// the dissipative flux and the update), primitives updated in place.
+void Engine::smoothed_iteration_body() {
+	save_w0(-1);
+	spectral_radius(-1);
+	timestep(-1);
+	for (size_t s = 0; s < alpha_.size(); s++) {
+		if (order_ == 2) {
+			gradients(-1, grad_kind_);
+			limiters(-1, lim_kind_, deck_.omega, deck_.k);
+		}
+		flux_conv(-1, scheme_);
+		flux_diss(-1, scheme_, beta_[s]);
+		smooth_residual(-1);
+		update_internal(-1, alpha_[s]);
+		update_boundary(-1);
+	}
+	double* prim = cur_ ? f64_.P1.p : f64_.P0.p;
+	double* other = cur_ ? f64_.P0.p : f64_.P1.p;
+	ReduceArgs a = make_reduce(NR_, NA_, nb_, roff_d_.p, chunk_, max_chunks_, partial_.p, wall_off_.p, wall_face_.p,
+	                           (int)wall_face_.n, wall_terms_.p, face_lr_.p, S_.p, fc_.p, denom_, hist_d_.p, iter_d_.p,
+	                           bad_d_.p);
+	a.wall_denom = wall_denom_d_.p;
+	launch_reduce<double>(a, f64_.Rc.p, f64_.Rd.p, prim, st_);
+	launch_halo<double>((int)halo_dst_.n, halo_dst_.p, halo_src_.p, NA_, prim, other, st_);
+	launch_iter_advance(iter_d_.p, st_);
+}
+
 template <class T>
 void Engine::iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* marks) {
+	if (deck_.smoothing) {
+		smoothed_iteration_body();
+		return;
+	}
 	const int stages = (int)alpha_.size();
 	auto mark = [&]() {
 		if (marks) {
@@ -689,6 +732,8 @@ void Engine::iteration_body(Fused<T>& f, int parity, std::vector<cudaEvent_t>* m
 
 int Engine::launches_per_iteration() const {
 	const int stages = (int)alpha_.size();
+	if (deck_.smoothing)  // W0, spectral radius, time step; per stage (grad, lim,) conv, diss, 2 smoothing, update, BC
+		return 3 + stages * ((order_ == 2 ? 2 : 0) + 6) + 3 + (halo_dst_.n ? 1 : 0) + 1;
 	return (order_ == 2 ? 2 * stages : stages + 1) + 3 /*reduce*/ + (halo_dst_.n ? 1 : 0) + 1 /*advance*/;
 }
 
@@ -713,7 +758,7 @@ void Engine::run_iterations(Fused<T>& f, int n) {
 				iteration_body<T>(f, cur_, nullptr);
 				check("iteration");
 			}
-			cur_ ^= (stages & 1);
+			cur_ ^= deck_.smoothing ? 0 : (stages & 1);
 		}
 		dev_iter_ += m;
 		n -= m;
@@ -755,7 +800,7 @@ double Engine::iterate_timed(int n) {
 			else iteration_body<float>(f32_, cur_, nullptr);
 			check("iteration");
 		}
-		cur_ ^= (stages & 1);
+		cur_ ^= deck_.smoothing ? 0 : (stages & 1);
 	}
 	cuda_ok(cudaEventRecord(e1, st_), "event");
 	cuda_ok(cudaEventSynchronize(e1), "event sync");
@@ -1107,6 +1152,7 @@ double Engine::bytes_flux(bool order1, bool diss, bool last) const {
 }
 
 std::vector<Engine::KernelTime> Engine::time_kernels(int n) {
+	if (deck_.smoothing) throw Error(E3D_ERR_STATE, "per-kernel timing covers the fused path (no residual smoothing)");
 	std::vector<KernelTime> out;
 	if (!started_) halo();
 	const int stages = (int)alpha_.size();

@@ -66,6 +66,7 @@ public:
 	void flux_diss(int block, int scheme, double beta);
 	void update_internal(int block, double alpha);
 	void update_boundary(int block);
+	void smooth_residual(int block);  // CentralIrsSmoother::smoothResidual
 	void halo();
 	// per-block norms and forces of the current state (PostProcessing::computeFlowData)
 	void flow_data(std::vector<double>& per_block10);
@@ -162,6 +163,7 @@ private:
 	template <class T>
 	void run_iterations(Fused<T>& f, int n);
 	void collect_history(int first_iter, int n);
+	void smoothed_iteration_body();
 	void block_range(int block, int& r0, int& r1, int& g0, int& g1) const;
 	void require_fp64(const char* what) const;
 	StateView state64();
@@ -227,6 +229,7 @@ private:
 	void autotune(int iters);
 	void snapshot(bool save);
 	DevBuf<unsigned char> snap_;
+	DevBuf<double> irs_;  // residual-smoothing Jacobi start values, 10 x NR
 	size_t dev_bytes_ = 0;
 };
 

@@ -58,6 +58,11 @@ void launch_bc(const GeoView& g, const StateView& s, const Physics& ph, int g0, 
 	if (g1 > g0) k_bc<<<blocks_for(g1 - g0, TPB), TPB, 0, st>>>(g, s, ph, g0, g1);
 }
 void launch_iter_advance(int* d_iter, cudaStream_t st) { k_iter_advance<<<1, 1, 0, st>>>(d_iter); }
+void launch_smooth(const GeoView& g, const StateView& s, double* j1, int r0, int r1, cudaStream_t st) {
+	if (r1 <= r0) return;
+	k_irs_start<<<blocks_for(r1 - r0, TPB), TPB, 0, st>>>(g, s, j1, r0, r1);
+	k_irs_smooth<<<blocks_for(r1 - r0, TPB), TPB, 0, st>>>(g, s, j1, r0, r1);
+}
 
 template void launch_halo<double>(int, const int*, const int*, int, double*, double*, cudaStream_t);
 template void launch_reduce<double>(const ReduceArgs&, const double*, const double*, const double*, cudaStream_t);

@@ -323,6 +323,47 @@ __global__ void k_bc(GeoView g, StateView s, Physics ph, int g0, int g1) {
 // per outer iteration (BlockCommunicator::updateBoundaries, serial path
 // MPI/src/BlockCommunicator.cpp:212-268; the other 35 copied values are
 // rewritten before any read).  Writes every buffer in `bufs`.
+// CentralIrsSmoother::smoothResidual (Solver/src/CentralIrsSmoother.cpp:12-166):
+// one Jacobi step of central implicit residual smoothing, eps = 0.8, applied to
+// the convective and the dissipative residuals of the real cells.  Pass 1: the
+// start value J1 = R / (1 + eps N) (N = the cell's face count) of all ten arrays.
+// The reference fills J1 of the dissipative v-momentum from the w-momentum and
+// never fills J1 of the dissipative w-momentum (:90); these two follow the
+// formula of the other eight here.
+constexpr double IRS_EPS = 0.8;
+__global__ void k_irs_start(GeoView g, StateView s, double* __restrict__ j1, int r0, int r1) {
+	const int c = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= r1) return;
+	const int na = g.slot_ptr[c + 1] - g.slot_ptr[c];
+	for (int q = 0; q < 5; q++) {
+		j1[q * (size_t)g.NR + c] = (s.rc[q * (size_t)g.NR + c] + 0.) / (1. + IRS_EPS * na);
+		j1[(5 + q) * (size_t)g.NR + c] = (s.rd[q * (size_t)g.NR + c] + 0.) / (1. + IRS_EPS * na);
+	}
+}
+
+// Pass 2: R = (R + eps * sum of J1 over the real neighbours in slot order) / (1 + eps N),
+// in place (each thread reads only its own R and the neighbours' J1).
+__global__ void k_irs_smooth(GeoView g, StateView s, const double* __restrict__ j1, int r0, int r1) {
+	const int c = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= r1) return;
+	double sc[5] = {0., 0., 0., 0., 0.}, sd[5] = {0., 0., 0., 0., 0.};
+	for (int k = g.slot_ptr[c]; k < g.slot_ptr[c + 1]; k++) {
+		const int nb = g.slot_nbr[k];
+		if (nb < g.NR)
+			for (int q = 0; q < 5; q++) {
+				sc[q] += j1[q * (size_t)g.NR + nb];
+				sd[q] += j1[(5 + q) * (size_t)g.NR + nb];
+			}
+	}
+	const int na = g.slot_ptr[c + 1] - g.slot_ptr[c];
+	for (int q = 0; q < 5; q++) {
+		double& rc = s.rc[q * (size_t)g.NR + c];
+		double& rd = s.rd[q * (size_t)g.NR + c];
+		rc = (rc + IRS_EPS * sc[q]) / (1. + IRS_EPS * na);
+		rd = (rd + IRS_EPS * sd[q]) / (1. + IRS_EPS * na);
+	}
+}
+
 template <class T>
 __global__ void k_halo(int n, const int* __restrict__ dst, const int* __restrict__ src, int NA, T* b0, T* b1) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;

@@ -20,6 +20,8 @@ void launch_flux_diss(const GeoView&, const StateView&, const Physics&, int sche
                       cudaStream_t);
 void launch_update(const GeoView&, const StateView&, const Physics&, double alpha, int r0, int r1, cudaStream_t);
 void launch_bc(const GeoView&, const StateView&, const Physics&, int g0, int g1, cudaStream_t);
+// central implicit residual smoothing of Rc and Rd (j1: 10 x NR FP64 scratch)
+void launch_smooth(const GeoView&, const StateView&, double* j1, int r0, int r1, cudaStream_t);
 
 // ---- shared by both paths, per precision ----
 template <class T>

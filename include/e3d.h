@@ -124,6 +124,13 @@ int e3d_flux_conv(e3d_solver* s, int block, int scheme);             /* FluxSche
 int e3d_flux_diss(e3d_solver* s, int block, int scheme, double beta);/* FluxScheme::computeFluxDiss, RoeScheme.cpp:12-311; AusmScheme.cpp:12-243 */
 int e3d_update_internal(e3d_solver* s, int block, double alpha);    /* Updater::updateInternalBlock, Updater.cpp:12-78 */
 int e3d_update_boundary(e3d_solver* s, int block);                   /* Updater::updateBoundary, Updater.cpp:80-88 */
+/* CentralIrsSmoother::smoothResidual, CentralIrsSmoother.cpp:12-166: one Jacobi
+ * step of central implicit residual smoothing (eps 0.8) of the convective and
+ * dissipative residuals of the real cells; the reference's dissipative v and w
+ * momentum start values (its lines 90-91 copy w into v and leave w unset)
+ * follow the formula of the other eight arrays here.  A deck with
+ * smoothing = 1 runs it in every stage of e3d_iterate / e3d_solve (FP64). */
+int e3d_smooth_residual(e3d_solver* s, int block);
 int e3d_halo(e3d_solver* s);                                         /* BlockCommunicator::updateBoundaries, MPI/src/BlockCommunicator.cpp:66-270 */
 /* PostProcessing::computeFlowData (PostProcessing.cpp:198-217) for every block:
  * out[b*10 + 0..4] = sum over real cells of (Rc-Rd)^2 per equation,

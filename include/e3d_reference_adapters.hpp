@@ -3,7 +3,7 @@
 //
 // Header-only C++ for maintainers of the reference code: compile it inside the
 // reference tree (it includes the reference's own headers FluxScheme.h,
-// Gradient.h, Limiter.h, Block.h, PrimitiveVariables.h, InterpolationVariables.h,
+// Gradient.h, Limiter.h, ResidualSmoother.h, Block.h, PrimitiveVariables.h, InterpolationVariables.h,
 // TimeVariables.h) and link libe3d.so.  Each class derives from, or has the same
 // methods as, the reference class it replaces and forwards to one entry point of
 // include/e3d.h on the device-resident copy of the same block (the reference's
@@ -22,6 +22,7 @@
 #include "InterpolationVariables.h"
 #include "Limiter.h"
 #include "PrimitiveVariables.h"
+#include "ResidualSmoother.h"
 #include "TimeVariables.h"
 #include "e3d.h"
 
@@ -93,6 +94,16 @@ public:
 class GpuVenkatakrishnan : public GpuLimiter {
 public:
 	GpuVenkatakrishnan(e3d_solver* s, double k) : GpuLimiter(s, E3D_LIM_VENKATAKRISHNAN, 0.0, k) {}
+};
+
+// ResidualSmoother (Solver/head/ResidualSmoother.h:8-18) -> CentralIrsSmoother
+class GpuCentralIrsSmoother : public ResidualSmoother {
+public:
+	explicit GpuCentralIrsSmoother(e3d_solver* s) : s_(s) {}
+	void smoothResidual(Block* b) override { check(e3d_smooth_residual(s_, b->block_id_), "smooth_residual"); }
+
+private:
+	e3d_solver* s_;
 };
 
 // Timestep (Solver/head/Timestep.h:10-27): same methods, device arrays

@@ -6,6 +6,7 @@
  * (file:line cited per function) so results are bit-identical to the
  * reference's x86-64 build.
  */
+#include <stdlib.h>
 #include "e3d_oracle.h"
 
 #include <math.h>
@@ -352,6 +353,46 @@ void e3d_oracle_update_internal(e3d_oracle_block* b, const e3d_oracle_params* p,
 /* Updater::updateBoundary (Updater.cpp:80-88): WallCellIds / SymmetryCellIds
  * (slip, DataStructure/src/WallCellIds.cpp:9-95, SymmetryCellIds.cpp:9-96),
  * FarfieldCellIds (characteristic, FarfieldCellIds.cpp:10-205); CONNEXION no-op */
+/* CentralIrsSmoother::smoothResidual (Solver/src/CentralIrsSmoother.cpp:12-166):
+ * J1 = R / (1 + eps Na) for every real cell (:78-91), then
+ * R = (R + eps * sum of J1 over the real neighbours in cell_2_cells order) / (1 + eps Na)
+ * (:92-142), eps = 0.8, Na = the cell's face count.  The reference sets the
+ * dissipative v start value from w and leaves w unset (:90); here both follow
+ * the formula of the other eight arrays. */
+void e3d_oracle_smooth(e3d_oracle_block* b) {
+	const int nr = b->n_real, na = b->n_all;
+	const double epsilon = 0.8;
+	double* j1 = (double*)malloc(sizeof(double) * 10 * (size_t)nr);
+	double* out = (double*)malloc(sizeof(double) * 10 * (size_t)nr);
+	for (int c = 0; c < nr; c++) {
+		const int Na = b->cell_face_ptr[c + 1] - b->cell_face_ptr[c];
+		for (int q = 0; q < 5; q++) {
+			j1[q * (size_t)nr + c] = (b->conv_res[q * (size_t)na + c] + 0.) / (1. + epsilon * Na);
+			j1[(5 + q) * (size_t)nr + c] = (b->diss_res[q * (size_t)na + c] + 0.) / (1. + epsilon * Na);
+		}
+	}
+	for (int c = 0; c < nr; c++) {
+		double sum[10] = {0., 0., 0., 0., 0., 0., 0., 0., 0., 0.};
+		for (int k = b->cell_face_ptr[c]; k < b->cell_face_ptr[c + 1]; k++) {
+			const int j = b->cell_cells[k];
+			if (j < nr)
+				for (int q = 0; q < 10; q++) sum[q] += j1[q * (size_t)nr + j];
+		}
+		const int Na = b->cell_face_ptr[c + 1] - b->cell_face_ptr[c];
+		for (int q = 0; q < 5; q++) {
+			out[q * (size_t)nr + c] = (b->conv_res[q * (size_t)na + c] + epsilon * sum[q]) / (1. + epsilon * Na);
+			out[(5 + q) * (size_t)nr + c] = (b->diss_res[q * (size_t)na + c] + epsilon * sum[5 + q]) / (1. + epsilon * Na);
+		}
+	}
+	for (int c = 0; c < nr; c++)
+		for (int q = 0; q < 5; q++) {
+			b->conv_res[q * (size_t)na + c] = out[q * (size_t)nr + c];
+			b->diss_res[q * (size_t)na + c] = out[(5 + q) * (size_t)nr + c];
+		}
+	free(j1);
+	free(out);
+}
+
 void e3d_oracle_update_boundary(e3d_oracle_block* b, const e3d_oracle_params* p) {
 	const int n = b->n_all;
 	double fr[5];
@@ -522,6 +563,7 @@ int e3d_oracle_iterate(e3d_oracle_block* blocks, int n_blocks, const e3d_oracle_
 				}
 				e3d_oracle_flux_conv(b, p);
 				e3d_oracle_flux_diss(b, p, beta[s]);
+				if (p->smoothing) e3d_oracle_smooth(b);
 				e3d_oracle_update_internal(b, p, alpha[s]);
 				e3d_oracle_update_boundary(b, p);
 			}

@@ -53,6 +53,7 @@ typedef struct e3d_oracle_block {
 typedef struct e3d_oracle_params {
 	double gamma, cfl, mach, aoa_deg, cmac, omega, k;
 	int stages, order, flux, gradient, limiter; /* flux 0 roe 1 ausm; gradient 0 GG 1 LS; limiter 0 BJ 1 V */
+	int smoothing; /* 1: central implicit residual smoothing in every stage */
 } e3d_oracle_params;
 
 /* one inter-block copy list (ConnexionCellIds) */
@@ -73,6 +74,8 @@ void e3d_oracle_flux_conv(e3d_oracle_block* b, const e3d_oracle_params* p);
 void e3d_oracle_flux_diss(e3d_oracle_block* b, const e3d_oracle_params* p, double beta);
 void e3d_oracle_update_internal(e3d_oracle_block* b, const e3d_oracle_params* p, double alpha);
 void e3d_oracle_update_boundary(e3d_oracle_block* b, const e3d_oracle_params* p);
+/* CentralIrsSmoother::smoothResidual; the dissipative v/w start values follow the other eight arrays */
+void e3d_oracle_smooth(e3d_oracle_block* b);
 void e3d_oracle_halo(e3d_oracle_block* blocks, const e3d_oracle_connexion* c, int n_connexions);
 /* out[0..4] = per-equation sum of (Rc-Rd)^2; out[5..9] = wall sums fy, fx, cmx, cmy, cmz */
 void e3d_oracle_flow_data(const e3d_oracle_block* b, const e3d_oracle_params* p, double out[10]);

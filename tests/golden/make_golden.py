@@ -70,6 +70,11 @@ CASES = {
                               iters=20, dump_iters=[1, 20]),
     "h5_o1_ausm": dict(kind="hex", n=5, nz=2, deck=dict(order=1, flux="ausm", mach=0.6, aoa_deg=3.0, cfl=0.5),
                        iters=20, dump_iters=[1, 20]),
+    # residual smoothing: only the first smoothed residual is comparable (the
+    # reference's dissipative w-momentum start value is never set)
+    "irs_t3_o1_roe_b2": dict(kind="tet", n=4, blocks=2, deck=dict(order=1, flux="roe", mach=0.5, aoa_deg=2.0,
+                                                                  smoothing=1),
+                             iters=1, dump_iters=[1]),
 }
 # Full-size history goldens (minutes of reference CPU time): --large
 LARGE = {

@@ -31,7 +31,8 @@ class OBlock(C.Structure):
 class OParams(C.Structure):
     _fields_ = [("gamma", C.c_double), ("cfl", C.c_double), ("mach", C.c_double), ("aoa_deg", C.c_double),
                 ("cmac", C.c_double), ("omega", C.c_double), ("k", C.c_double), ("stages", C.c_int),
-                ("order", C.c_int), ("flux", C.c_int), ("gradient", C.c_int), ("limiter", C.c_int)]
+                ("order", C.c_int), ("flux", C.c_int), ("gradient", C.c_int), ("limiter", C.c_int),
+                ("smoothing", C.c_int)]
 
 
 class OConn(C.Structure):
@@ -112,7 +113,7 @@ def params_from_deck(d) -> OParams:
     else:
         flux, grad, lim = d.flux, d.gradient, d.limiter
     return OParams(get("gamma"), get("cfl"), get("mach"), get("aoa_deg"), get("cmac"), get("omega"), get("k"),
-                   get("stages"), get("order"), flux, grad, lim)
+                   get("stages"), get("order"), flux, grad, lim, int(bool(get("smoothing"))))
 
 
 class OracleCase:
