@@ -591,8 +591,12 @@ __device__ __forceinline__ void recon_cell(const FusedView<T>& v, const Physics&
 	}
 }
 
+// resident blocks per SM the FP32 reconstruction pass is compiled for (8: 64 registers)
+#ifndef E3D_RECON_MIN_BLOCKS
+#define E3D_RECON_MIN_BLOCKS 8
+#endif
 template <class T, int GRAD, int LIM, bool FIRST, int NSL>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_recon(FusedView<T> v, Physics ph, int carry_w0) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? E3D_RECON_MIN_BLOCKS : 4) k_recon(FusedView<T> v, Physics ph, int carry_w0) {
 	const int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c < v.NR) recon_cell<T, GRAD, LIM, FIRST, NSL>(v, ph, carry_w0, c);
 }
