@@ -464,7 +464,7 @@ def main():
 
         # per-kernel device times (eager launches with events between kernels)
         kt = s.time_kernels(min(steps, 10))
-        dom = max(kt, key=lambda k: k["total_ms"])
+        dom = max((k for k in kt if k["bytes_per_launch"]), key=lambda k: k["total_ms"])
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
