@@ -83,14 +83,15 @@ def solve_plain(case: api.Case, criterion: float, max_iter: int, check_every: in
 
 
 def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrogate: api.Surrogate | None = None,
-                  switch_at: float | None = -4.5, iters_per_launch: int = 50, stall_window: int = 3000,
+                  switch_at: float | None = -5.0, iters_per_launch: int = 50, stall_window: int = 400,
                   fp64: str = "fp64-fma") -> dict:
     """All cases in one batch: one freestream iteration (the reference residual
     of each case's drop), the surrogate's warm start when given, FP32
-    iterations to `switch_at` (a case stalled for `stall_window` iterations
-    also moves on), then FP64 iterations to `criterion` (`fp64`: "fp64-fma"
-    for the kernels built with fused multiply-add, "fp64" for the
-    bit-identical ones); each case leaves the work list once it gets there."""
+    iterations to `switch_at` (a case whose FP32 residual has stopped falling
+    for `stall_window` iterations, its FP32 rounding floor, also moves on),
+    then FP64 iterations to `criterion` (`fp64`: "fp64-fma" for the kernels
+    built with fused multiply-add, "fp64" for the bit-identical ones); each
+    case leaves the work list once it gets there."""
     t0 = time.perf_counter()
     b = api.Batch(cases, precision="fp32" if switch_at is not None else "fp64",
                   hist_capacity=max(4096, iters_per_launch * 4))
