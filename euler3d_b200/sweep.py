@@ -87,8 +87,9 @@ def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrog
                   fp64: str = "fp64-fma") -> dict:
     """All cases in one batch: one freestream iteration (the reference residual
     of each case's drop), the surrogate's warm start when given, FP32
-    iterations to `switch_at` (a case whose FP32 residual has stopped falling
-    for `stall_window` iterations, its FP32 rounding floor, also moves on),
+    iterations to `switch_at` (below a 4-order drop, a case whose FP32
+    residual has stopped falling for `stall_window` iterations, its FP32
+    rounding floor, also moves on),
     then FP64 iterations to `criterion` (`fp64`: "fp64-fma" for the kernels
     built with fused multiply-add, "fp64" for the bit-identical ones); each
     case leaves the work list once it gets there."""
@@ -109,6 +110,9 @@ def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrog
     phases = []
     if switch_at is not None:
         tp = time.perf_counter()
+        # stall detection only near the floor: the early transient of a freestream
+        # start has plateaus of its own
+        b.solve_batch(max_iter, max(switch_at, -4.0), iters_per_launch=iters_per_launch)
         b.solve_batch(max_iter, switch_at, iters_per_launch=iters_per_launch, stall_window=stall_window)
         phases.append(dict(precision="fp32", to=switch_at, wall_s=time.perf_counter() - tp, tuning=b.tuning()))
         tp = time.perf_counter()
