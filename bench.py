@@ -82,6 +82,44 @@ def wing_case(a, td):
     return os.path.join(case_dir, "wing.deck"), case_dir, cfg
 
 
+def fp32_error_report(td):
+    """The FP32 variant's error against the FP64 path, which is the reference's
+    arithmetic bit for bit: the 20^3 x 6 (48,000-tet) first-order Roe case, M 0.5,
+    500 iterations, and the first 20 iterations of the 3.07M-tet second-order
+    workload's own scheme on a 20^3 x 6 mesh in 4 blocks."""
+    import numpy as np
+
+    from euler3d_b200 import api
+    from euler3d_b200 import meshgen as mg
+
+    out = {}
+    cases = {"bump20_o1_roe_500it": (20, 1, dict(order=1, flux="roe", mach=0.5, aoa_deg=0.0), 500),
+             "bump20b4_o2_ls_venk_roe_20it": (20, 4, dict(order=2, flux="roe", gradient="leastsquares",
+                                                          limiter="venkatakrishnan", k=5.0, mach=0.7,
+                                                          aoa_deg=1.25), 20)}
+    for name, (n, nb, deck, iters) in cases.items():
+        path = mg.write_case(os.path.join(td, "err_" + name), n, nb, deck=mg.Deck(topology="", **deck))
+        case = api.Case(path)
+        res = {}
+        for prec in ("fp64", "fp32"):
+            s = api.Solver(case, precision=prec, hist_capacity=iters + 16)
+            s.iterate(iters)
+            res[prec] = (s.history(), [s.get(b, "prim") for b in range(case.n_blocks)])
+            s.close()
+        h64, p64 = res["fp64"]
+        h32, p32 = res["fp32"]
+        scale = np.array([1.0, 0.7 * 1.4 ** 0.5, 0.7 * 1.4 ** 0.5, 0.7 * 1.4 ** 0.5, 1.0])  # freestream magnitudes
+        dev = max(float(np.max(np.abs(a.reshape(5, -1) - b.reshape(5, -1)) / scale[:, None])) for a, b in zip(p32, p64))
+        out[name] = {"iterations": iters,
+                     "max_abs_ro_conv_decades": float(np.max(np.abs(h32["conv"][:, 0] - h64["conv"][:, 0]))),
+                     "cl_rel": float(abs(h32["cl"][-1] - h64["cl"][-1]) / abs(h64["cl"][-1])),
+                     "cd_rel": float(abs(h32["cd"][-1] - h64["cd"][-1]) / abs(h64["cd"][-1])),
+                     "max_cell_state_dev": dev,
+                     "note": "state deviation scaled by freestream density, speed and pressure"}
+        case.close()
+    return out
+
+
 def workload_config(n, blocks, precision):
     w = WORKLOAD
     return {"workload": f"bump channel {n}^3 hex x 6 tets ({6 * n ** 3:,} tets), {blocks} slab blocks on one GPU, "
@@ -520,6 +558,9 @@ def main():
         # timestamp in this query: keep all samples of the measured run)
         cl = ClockSampler.summarize(rows)
 
+        fp32_err = None
+        if rank == 0 and a.precision == "fp32" and a.workload == "channel":
+            fp32_err = fp32_error_report(td)
         cpu = None
         if rank == 0 and world == 1 and not a.no_cpu_baseline:
             try:
@@ -534,7 +575,8 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": cl,
             "final": {"iterations": int(len(hist["iter"])), "ro_conv": float(hist["conv"][-1, 0]),
-                      "cl": float(hist["cl"][-1]), "cd": float(hist["cd"][-1])}}
+                      "cl": float(hist["cl"][-1]), "cd": float(hist["cd"][-1])},
+            "fp32_vs_fp64": fp32_err}
     if rank == 0:
         print(json.dumps(line))
     s.close()
