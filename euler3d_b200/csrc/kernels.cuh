@@ -452,6 +452,30 @@ __device__ __forceinline__ void load_geo(const T* __restrict__ a, const SlotRang
 // Pass 1 of a stage, one thread per real cell: gradient, limiter and MUSCL
 // face states of the cell and of its ghost cells.  FIRST additionally computes
 // W0 (unless carried) and the local time step from the stage-0 state.
+// first stage only: W0 (unless carried) and the local time step (Timestep.cpp:26-148)
+template <class T, int NSL>
+__device__ __forceinline__ void first_stage_extras(const FusedView<T>& v, const Physics& ph, int carry_w0, int c) {
+	const SlotRange<T, NSL> sr(v, c);
+	const Q5<T> q0 = ld5(v.Pin, v.NA, c);
+	const T V = v.vol[c];
+	if (!carry_w0) {
+		const int n = v.NR;
+		v.W0[c] = (double)q0.r;
+		v.W0[n + c] = (double)(q0.r * q0.u);
+		v.W0[2 * n + c] = (double)(q0.r * q0.v);
+		v.W0[3 * n + c] = (double)(q0.r * q0.w);
+		v.W0[4 * n + c] = (double)(T(0.5) * q0.r * (q0.u * q0.u + q0.v * q0.v + q0.w * q0.w) +
+		                           T(1.) / (T(ph.gamma) - T(1.0)) * q0.p);
+	}
+	T geo[MAXSL][4];
+	load_geo<T, NSL>(v.sgeo, sr, geo);
+	const T cc = tsqrt(T(ph.gamma) * q0.p / q0.r);
+	T srad = T(0.0);
+#pragma unroll
+	E3D_SLOTS(k, sr) srad += (tabs((q0.u) * geo[k][0] + (q0.v) * geo[k][1] + (q0.w) * geo[k][2]) + (cc)) * geo[k][3];
+	v.dt[c] = T(ph.cfl) * V / srad;
+}
+
 template <class T, int GRAD, int LIM, bool FIRST, int NSL>
 __device__ __forceinline__ void recon_cell(const FusedView<T>& v, const Physics& ph, int carry_w0, int c) {
 	const SlotRange<T, NSL> sr(v, c);
@@ -571,24 +595,7 @@ __device__ __forceinline__ void recon_cell(const FusedView<T>& v, const Physics&
 			st5(v.FS, v.NS, ms, fs);
 		}
 	}
-	if (FIRST) {
-		if (!carry_w0) {
-			const int n = v.NR;
-			v.W0[c] = (double)q0.r;
-			v.W0[n + c] = (double)(q0.r * q0.u);
-			v.W0[2 * n + c] = (double)(q0.r * q0.v);
-			v.W0[3 * n + c] = (double)(q0.r * q0.w);
-			v.W0[4 * n + c] = (double)(T(0.5) * q0.r * (q0.u * q0.u + q0.v * q0.v + q0.w * q0.w) +
-			                           T(1.) / (T(ph.gamma) - T(1.0)) * q0.p);
-		}
-		T geo[MAXSL][4];
-		load_geo<T, NSL>(v.sgeo, sr, geo);
-		const T cc = tsqrt(T(ph.gamma) * q0.p / q0.r);
-		T srad = T(0.0);
-#pragma unroll
-		E3D_SLOTS(k, sr) srad += (tabs((q0.u) * geo[k][0] + (q0.v) * geo[k][1] + (q0.w) * geo[k][2]) + (cc)) * geo[k][3];
-		v.dt[c] = T(ph.cfl) * V / srad;
-	}
+	if (FIRST) first_stage_extras<T, NSL>(v, ph, carry_w0, c);
 }
 
 // resident blocks per SM the FP32 reconstruction pass is compiled for (8: 64 registers)
