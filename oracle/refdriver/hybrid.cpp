@@ -71,7 +71,8 @@ int main(int argc, char** argv) {
 	check(e3d_solver_create(ec, &opt, &es), "solver_create");
 
 	// strategy objects selected by the reference's strings (ResidualCalculator.cpp:72-95,
-	// SecondOrder.cpp:50-61), RK tables of RungeKutta.cpp:23-68 taken from its objects
+	// SecondOrder.cpp:50-61) and the smoother (ResidualCalculator.cpp:90-93), RK tables of
+	// RungeKutta.cpp:23-68 taken from its objects
 	const double gamma = interface->gamma_interface_;
 	FluxScheme* flux = interface->flux_scheme_choice_interface_ == "ausm"
 	                       ? static_cast<FluxScheme*>(new GpuAusmScheme(es, gamma))
@@ -85,6 +86,8 @@ int main(int argc, char** argv) {
 		if (interface->limiter_choice_interface_ == "venkatakrishnan") lim = new GpuVenkatakrishnan(es, interface->k_interface_);
 		else lim = new GpuBarthJespersen(es, interface->omega_interface_);
 	}
+	ResidualSmoother* smoother = nullptr;
+	if (interface->residual_smoother_choice_interface_) smoother = new GpuCentralIrsSmoother(es);
 	GpuTimestep ts(es, gamma, interface->cfl_interface_);
 	const std::vector<double> beta = solver->runge_kutta_->residual_calculator_->beta_rk_;
 	GpuUpdater up(es, gamma, solver->runge_kutta_->updater_->alpha_rk_);
@@ -108,6 +111,7 @@ int main(int argc, char** argv) {
 				flux->computeFluxConv(b);
 				flux->current_beta_ = beta[s];
 				flux->computeFluxDiss(b);
+				if (smoother) smoother->smoothResidual(b);
 				up.current_stage_ = s;
 				up.updateInternalBlock(b);
 				up.updateBoundary(b);

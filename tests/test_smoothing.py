@@ -133,3 +133,28 @@ def test_smoothing_deck_runs_fused_and_matches_the_oracle(tmp_path):
         assert same(pa, oc.blocks[blk].prim)
     with pytest.raises(Exception):
         api.Solver(case, precision="fp32")  # the smoother runs on the FP64 path
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not __import__("os").path.exists(
+    __import__("os").path.join(__import__("conftest").REPO, "oracle", "_ref", "e3d_hybrid")),
+    reason="e3d_hybrid not built (reference sources absent at build)")
+def test_reference_loop_with_the_gpu_smoother(tmp_path):
+    """The reference's own outer loop and post-processing with GpuCentralIrsSmoother
+    (and the other GPU strategies) plugged in: the history equals the fused path's."""
+    import os
+    import subprocess
+
+    from conftest import REPO
+
+    g = Golden(NAME)
+    deck = g.write_case(str(tmp_path))
+    hist = os.path.join(tmp_path, "h.csv")
+    subprocess.run([os.path.join(REPO, "oracle", "_ref", "e3d_hybrid"), os.path.basename(deck), "--iters", "6",
+                    "--history", hist], cwd=tmp_path, check=True, capture_output=True, timeout=600)
+    h = np.genfromtxt(hist, delimiter=",", names=True)
+    s = api.Solver(api.Case(deck), precision="fp64")
+    s.iterate(6)
+    ours = s.history()
+    assert same(h["cl"], ours["cl"]) and same(h["cd"], ours["cd"])
+    assert np.max(np.abs(h["rms_ro"] - ours["rms"][:, 0]) / np.abs(h["rms_ro"])) < 1e-12
