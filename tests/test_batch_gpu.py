@@ -184,3 +184,21 @@ def test_batch_rejects_mixed_settings_and_hex_meshes(tmp_path):
     with pytest.raises(E3DError):
         b.solve_batch(2, NEVER)
     b.iterate(2)  # the per-pass path covers mixed-element meshes
+
+
+def test_stalled_case_leaves_the_work_list(tmp_path):
+    """A case whose residual stops falling (first-order Roe on the bump box with
+    farfield side faces stalls near 2-4 orders) leaves the batch after the stall
+    window; a channel case beside it keeps going to the criterion."""
+    d1 = mg.Deck(topology="", mach=0.5, aoa_deg=2.0, **O1_ROE)
+    stall = api.Case(mg.write_case(str(tmp_path / "s"), 6, 1, prefix="s", deck=d1, sides="farfield"))
+    d2 = mg.Deck(topology="", mach=0.5, aoa_deg=2.0, **O1_ROE)
+    conv = api.Case(mg.write_case(str(tmp_path / "c"), 6, 1, prefix="c", deck=d2, sides="channel"))
+    b = api.Batch([stall, conv], precision="fp64", hist_capacity=8192)
+    done, _ = b.solve_batch(30000, -7.0, iters_per_launch=100, stall_window=1500)
+    hs, hc = b.case_history(0)["conv"][:, 0], b.case_history(1)["conv"][:, 0]
+    assert hc.min() <= -7.0 and done[1] == int(np.argmax(hc <= -7.0)) + 1
+    assert hs.min() > -7.0 and len(hs) < 30000
+    # the stalled case stopped within one launch of the first window without a new minimum
+    best = np.minimum.accumulate(hs)
+    assert best[-1] > best[-1501] - 0.05
