@@ -598,12 +598,16 @@ __device__ __forceinline__ void recon_cell(const FusedView<T>& v, const Physics&
 	if (FIRST) first_stage_extras<T, NSL>(v, ph, carry_w0, c);
 }
 
-// resident blocks per SM the FP32 reconstruction pass is compiled for (8: 64 registers)
+// resident blocks per SM the FP32 reconstruction pass is compiled for (8: 64
+// registers) and the FP64 stage passes (4: 128 registers)
 #ifndef E3D_RECON_MIN_BLOCKS
 #define E3D_RECON_MIN_BLOCKS 8
 #endif
+#ifndef E3D_FP64_MIN_BLOCKS
+#define E3D_FP64_MIN_BLOCKS 4
+#endif
 template <class T, int GRAD, int LIM, bool FIRST, int NSL>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? E3D_RECON_MIN_BLOCKS : 4) k_recon(FusedView<T> v, Physics ph, int carry_w0) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? E3D_RECON_MIN_BLOCKS : E3D_FP64_MIN_BLOCKS) k_recon(FusedView<T> v, Physics ph, int carry_w0) {
 	const int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c < v.NR) recon_cell<T, GRAD, LIM, FIRST, NSL>(v, ph, carry_w0, c);
 }
@@ -737,7 +741,7 @@ __device__ __forceinline__ void flux_update_cell(const FusedView<T>& v, const Ph
 }
 
 template <class T, int SCHEME, bool ORDER1, int NSL, bool DISS>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4) k_flux_update(FusedView<T> v, Physics ph, T alpha, T beta, int last, int carry_w0) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : E3D_FP64_MIN_BLOCKS) k_flux_update(FusedView<T> v, Physics ph, T alpha, T beta, int last, int carry_w0) {
 	const int c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c < v.NR) flux_update_cell<T, SCHEME, ORDER1, NSL, DISS>(v, ph, alpha, beta, last, carry_w0, c);
 }
