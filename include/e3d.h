@@ -161,17 +161,18 @@ int e3d_state_set(e3d_solver* s, int block, const char* name, const double* src,
  * No counterpart in the reference (one case per run).  e3d_batch_create puts
  * every block of every case in one device arena; the cases must share gamma,
  * CFL, RK stages and the strategy choices and may differ in mesh, Mach, alpha
- * and chord.  e3d_batch_solve advances all cases together with the persistent
- * cooperative kernel (FP32 variant, tetrahedral meshes): one graph-captured
- * launch runs `iters_per_launch` outer iterations over a work list of tiles;
- * a case leaves the work list once its density drop reaches `criterion`, it
- * has run max_iter iterations in all, or (stall_window > 0) its last
- * stall_window iterations brought no new minimum 0.05 decades below the
- * earlier ones.  The first call autotunes the tile size and
- * the form: the persistent cooperative kernel with a tuned grid, or the same
- * phases as separate per-pass launches over the tiles in one captured graph
+ * and chord.  e3d_batch_solve (all-tetrahedron meshes; FP32 or FP64) advances
+ * the cases together over a work list of tiles, `iters_per_launch` outer
+ * iterations per graph launch; a case leaves the work list once its density
+ * drop reaches `criterion`, it has run max_iter iterations in all, or
+ * (stall_window > 0) its last stall_window iterations brought no new minimum
+ * 0.05 decades below the earlier ones.  The first call autotunes the form and
+ * the tile size: the persistent cooperative kernel with a tuned grid, or the
+ * same phases as per-pass launches over the tiles captured in one graph
  * (cached per problem-size bucket, and in $E3D_AUTOTUNE_CACHE if set;
- * e3d_batch_tuning reports *grid = 0 for the per-pass form).
+ * E3D_BATCH_FORM=persistent|per-pass forces a form; e3d_batch_tuning reports
+ * *grid = 0 for the per-pass form).  The tuning runs on a saved copy of the
+ * state, which is restored: it never changes the solution.
  * iters_done[c] = iterations case c needed (n_cases entries);
  * *device_ms = device time of the whole solve.  e3d_iterate also works on a
  * batch (every case advances; no per-case stop). */
