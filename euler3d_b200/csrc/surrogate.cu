@@ -514,8 +514,8 @@ void Surrogate::ensure_work(int n) {
 	part_.alloc((size_t)64 * (H * H + S::OUT * H + S::OUT));
 }
 
-// forward of n prepared rows (x_ filled)
-void Surrogate::forward(const float*, int, int n, bool) {
+// forward of n prepared rows (x_ filled): z1..z3, a1..a3, y
+void Surrogate::forward(int n) {
 	Epi e{};
 	e.ldo = H;
 	e.bias = master_.p + S::OFF_B1;
@@ -534,8 +534,8 @@ void Surrogate::forward(const float*, int, int n, bool) {
 	ok(cudaGetLastError(), "forward");
 }
 
-// backward of the rows of the last forward against targets t_; fills grad_ (all parameters)
-void Surrogate::backward(const float*, int, int n, double* loss_out) {
+// backward of the rows of the last forward against the targets in t_: loss and grad_ (all parameters)
+void Surrogate::backward(int n, double* loss_out) {
 	float* d4 = reinterpret_cast<float*>(g1_.p);  // reuse: d4 [n][OUT] floats fit in g1 ([n][H] BF16)
 	const int lb = blocks(n, 256);
 	k_loss<<<lb, 256, 0, st_>>>(n, y_.p, t_.p, d4, lossp_.p);
@@ -589,8 +589,8 @@ double Surrogate::train(int steps, int batch, double lr, std::vector<float>* los
 	for (int s = 0; s < steps; s++) {
 		k_prepare<<<blocks(batch, 256), 256, 0, st_>>>(batch, feat_.p, 8, state_.p, 8, n_samples_, seed_, step_,
 		                                               norm_.p, (float)gamma_, x_.p, t_.p);
-		forward(nullptr, 0, batch, true);
-		backward(nullptr, 0, batch, nullptr);
+		forward(batch);
+		backward(batch, nullptr);
 		ok(cudaMemcpyAsync(hist.p + s, loss_d_.p, sizeof(double), cudaMemcpyDeviceToDevice, st_), "loss");
 		step_++;
 		// cosine decay to 5% of lr over this call
@@ -623,9 +623,9 @@ double Surrogate::gradient(const float* feat6, const float* state5, int n, std::
 	sd.upload(s);
 	ensure_work(n);
 	k_prepare<<<blocks(n, 256), 256, 0, st_>>>(n, fd.p, 8, sd.p, 8, 0, 0, 0, norm_.p, (float)gamma_, x_.p, t_.p);
-	forward(nullptr, 0, n, true);
+	forward(n);
 	double loss = 0.0;
-	backward(nullptr, 0, n, &loss);
+	backward(n, &loss);
 	grad.resize(S::N_PARAM);
 	ok(cudaMemcpyAsync(grad.data(), grad_.p, S::N_PARAM * sizeof(float), cudaMemcpyDeviceToHost, st_), "grad");
 	ok(cudaStreamSynchronize(st_), "sync");
@@ -640,7 +640,7 @@ void Surrogate::predict_device(const float* feat, long long n, float* state, cud
 		const int m = (int)std::min<long long>(chunk, n - b0);
 		k_prepare<<<blocks(m, 256), 256, 0, st_>>>(m, feat + b0 * 8, 8, nullptr, 0, 0, 0, 0, norm_.p, (float)gamma_,
 		                                           x_.p, nullptr);
-		forward(nullptr, 0, m, false);
+		forward(m);
 		k_denormalise<<<blocks(m, 256), 256, 0, st_>>>(m, y_.p, feat + b0 * 8, 8, norm_.p, (float)gamma_,
 		                                               state + b0 * 8, 8);
 	}

@@ -7,7 +7,7 @@
 // are standardised with the mean and standard deviation of the training set.
 // Output: the conservative state (rho, rho u, rho v, rho w, rho E) as
 // W = W_free(Mach, alpha) + scale * y, where y is the network output and scale
-// the per-component standard deviation of W - W_free over the training set.
+// the per-component RMS of W - W_free over the training set.
 // No part of this has a counterpart in the reference solver.
 #pragma once
 #include <cstdint>
@@ -64,8 +64,8 @@ public:
 private:
 	void fit_normalisation();
 	void upload_params();
-	void forward(const float* feat_raw, int ld, int n, bool keep);  // into act buffers (n <= cap_)
-	void backward(const float* state_raw, int ld, int n, double* loss_out);
+	void forward(int n);                         // rows prepared in x_ (n <= work_n_)
+	void backward(int n, double* loss_out);      // against the targets in t_
 	void ensure_work(int n);
 
 	int device_;
