@@ -226,6 +226,10 @@ def run_reference_arm(a, rank: int):
     every block.  Bounded: at most 5 timed steps after at most 1 warm-up."""
     if rank != 0:
         return 0
+    if a.workload != "channel":
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference arm times the default workload; the "
+                                                             f"{a.workload} line carries its own cpu_baseline"}))
+        return 0
     n, blocks = a.n, a.blocks
     if not os.path.exists(REFDRIVER):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/e3d_refdriver was not built (the "
