@@ -131,6 +131,7 @@ Engine::Engine(const std::vector<const HostCase*>& cases, const EngineOptions& o
 	rms0_.assign(ncases_, {0, 0, 0, 0, 0});
 	hist_case_.assign(ncases_, {});
 	case_active_.assign(ncases_, 1);
+	case_failed_.assign(ncases_, 0);
 
 	if (opt_.stream) {
 		st_ = opt_.stream;
@@ -918,6 +919,28 @@ void Engine::collect_history(int first_iter, int n) {
 		}
 	}
 	total_iter_ += n;
+	if (bad && tolerate_nonfinite_) {
+		// a batch solve drops the cases whose residual turned non-finite and goes on
+		int failed = 0, alive = 0;
+		for (int cs = 0; cs < ncases_; cs++) {
+			if (!case_active_[cs]) continue;
+			const auto& hc = hist_case_[cs];
+			bool ok = true;
+			for (int i = std::max(0, (int)hc.size() - n); i < (int)hc.size(); i++)
+				for (int q = 0; q < 5; q++) ok = ok && std::isfinite(hc[i].rms[q]);
+			if (!ok) {
+				case_failed_[cs] = 1;
+				case_active_[cs] = 0;
+				failed++;
+			} else {
+				alive++;
+			}
+		}
+		if (failed > 0 && alive > 0) {
+			cuda_ok(cudaMemsetAsync(bad_d_.p, 0, sizeof(int), st_), "memset");
+			bad = 0;
+		}
+	}
 	if (bad) throw Error(E3D_ERR_NONFINITE, "non-finite residual norm by iteration " + std::to_string(total_iter_ - 1));
 }
 
@@ -1416,6 +1439,8 @@ void Engine::snapshot(bool save) {
 			cuda_ok(cudaMemcpyAsync(save ? (void*)q.bak : q.dev, save ? q.dev : (void*)q.bak, q.n,
 			                        cudaMemcpyDeviceToDevice, st_),
 			        "snapshot");
+	// a trial that met a non-finite state leaves no flag behind: the restored state is the one before
+	if (!save) cuda_ok(cudaMemsetAsync(bad_d_.p, 0, sizeof(int), st_), "memset");
 }
 
 // Picks the tile size (cells per work item) and the grid (resident blocks per
@@ -1498,7 +1523,12 @@ double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch,
 	if (iters_per_launch < 1) iters_per_launch = 1;
 	if (!started_) halo();
 	collect_history(total_iter_, dev_iter_);
-	std::fill(case_active_.begin(), case_active_.end(), 1);
+	struct Tolerate {
+		bool& flag;
+		explicit Tolerate(bool& f) : flag(f) { flag = true; }
+		~Tolerate() { flag = false; }
+	} tolerate(tolerate_nonfinite_);
+	for (int c = 0; c < ncases_; c++) case_active_[c] = case_failed_[c] ? 0 : 1;
 	double ms_total = 0.0;
 	auto update_active = [&]() {
 		bool changed = false;
@@ -1553,6 +1583,10 @@ double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch,
 	}
 	iters_done.assign(ncases_, 0);
 	for (int c = 0; c < ncases_; c++) {
+		if (case_failed_[c]) {
+			iters_done[c] = -1;
+			continue;
+		}
 		const auto& h = hist_case_[c];
 		int n = (int)h.size();
 		for (int i = 0; i < (int)h.size(); i++)
@@ -1562,7 +1596,7 @@ double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch,
 			}
 		iters_done[c] = n;
 	}
-	std::fill(case_active_.begin(), case_active_.end(), 1);
+	for (int c = 0; c < ncases_; c++) case_active_[c] = case_failed_[c] ? 0 : 1;
 	return ms_total;
 }
 

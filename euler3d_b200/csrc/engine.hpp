@@ -212,7 +212,8 @@ private:
 	std::vector<std::vector<IterRecord>> hist_case_;
 	cudaGraphExec_t graph_[2] = {nullptr, nullptr};
 	// batch (persistent kernel) state
-	std::vector<char> case_active_;
+	std::vector<char> case_active_, case_failed_;  // failed: residual turned non-finite in a batch solve
+	bool tolerate_nonfinite_ = false;
 	DevBuf<int> work_d_, block_work_d_;
 	DevBuf<double> wpart_d_;
 	int n_work_ = 0, tile_mult_ = 1, grid_ = 0;

@@ -173,6 +173,9 @@ int e3d_state_set(e3d_solver* s, int block, const char* name, const double* src,
  * E3D_BATCH_FORM=persistent|per-pass forces a form; e3d_batch_tuning reports
  * *grid = 0 for the per-pass form).  The tuning runs on a saved copy of the
  * state, which is restored: it never changes the solution.
+ * A case whose residual turns non-finite leaves the batch (iters_done[c] =
+ * -1, and later e3d_batch_solve calls skip it); the others go on, and the
+ * call fails with E3D_ERR_NONFINITE only when no case is left.
  * iters_done[c] = iterations case c needed (n_cases entries);
  * *device_ms = device time of the whole solve.  e3d_iterate also works on a
  * batch (every case advances; no per-case stop). */

@@ -202,3 +202,29 @@ def test_stalled_case_leaves_the_work_list(tmp_path):
     # the stalled case stopped within one launch of the first window without a new minimum
     best = np.minimum.accumulate(hs)
     assert best[-1] > best[-1501] - 0.05
+
+
+def test_non_finite_case_leaves_the_batch(tmp_path):
+    """A case whose state turns non-finite (here: a negative density planted on
+    the host) is dropped with iters_done = -1; the other cases are unaffected
+    and match their single-case solves bit for bit."""
+    cases = _cases(tmp_path, O1_ROE, sweep=SWEEP[:3])
+    batch = api.Batch(cases, precision="fp64")
+    prim = batch.get(0, "prim")
+    prim[0] = -1.0  # density of cell 0 of case 0
+    batch.set(0, "prim", prim)
+    done, _ = batch.solve_batch(8, NEVER, iters_per_launch=4)
+    assert done[0] == -1 and list(done[1:]) == [8, 8]
+    fb = cases[0].n_blocks
+    for c, case in enumerate(cases[1:], start=1):
+        _check_case(batch, c, fb, _single(case, "fp64", 8))
+        fb += case.n_blocks
+    done2, _ = batch.solve_batch(12, NEVER, iters_per_launch=4)
+    assert done2[0] == -1 and list(done2[1:]) == [12, 12]
+    # a batch with no case left reports the failure
+    solo = api.Batch(cases[:1], precision="fp64")
+    p0 = solo.get(0, "prim")
+    p0[0] = -1.0
+    solo.set(0, "prim", p0)
+    with pytest.raises(E3DError):
+        solo.solve_batch(4, NEVER, iters_per_launch=2)
