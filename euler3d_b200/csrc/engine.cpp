@@ -1578,8 +1578,13 @@ double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch,
 			}
 		if (!any || room <= 0) break;
 		ms_total += run_persistent(std::min(iters_per_launch, room));
+		const auto n_failed = [&]() { return std::count(case_failed_.begin(), case_failed_.end(), 1); };
+		const auto failed_before = n_failed();
 		collect_history(total_iter_, dev_iter_);
-		if (update_active()) build_work();
+		// a case dropped for a non-finite residual leaves the work list too, else its
+		// tiles run on and raise the flag again with no active case to claim it
+		const bool dropped = n_failed() != failed_before;
+		if (update_active() || dropped) build_work();
 	}
 	iters_done.assign(ncases_, 0);
 	for (int c = 0; c < ncases_; c++) {
