@@ -734,7 +734,10 @@ __device__ __forceinline__ void flux_update_cell(const FusedView<T>& v, const Ph
 				fr.v = T(f[2]);
 				fr.w = T(f[3]);
 				fr.p = T(f[4]);
-				st5(v.Pout, v.NA, nb[k], ghost_state(kind, qnew, fr, geo[k][0], geo[k][1], geo[k][2], g));
+				// the face normal is read again here (boundary slots only) so that the
+				// slots' geometry need not stay live through the update
+				const T* n = v.sgeo + 4 * (size_t)(sr.s0 + k);
+				st5(v.Pout, v.NA, nb[k], ghost_state(kind, qnew, fr, n[0], n[1], n[2], g));
 			}
 		}
 	}
