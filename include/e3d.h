@@ -178,7 +178,8 @@ int e3d_state_set(e3d_solver* s, int block, const char* name, const double* src,
  * call fails with E3D_ERR_NONFINITE only when no case is left.
  * iters_done[c] = iterations case c needed (n_cases entries);
  * *device_ms = device time of the whole solve.  e3d_iterate also works on a
- * batch (every case advances; no per-case stop). */
+ * batch (every case advances; no per-case stop), so after a case has left the
+ * batch it fails with E3D_ERR_NONFINITE: that case's state stays non-finite. */
 int e3d_batch_create(const e3d_case* const* cases, int n_cases, const e3d_options* opt, e3d_solver** out);
 int e3d_batch_solve(e3d_solver* s, int max_iter, double criterion, int iters_per_launch, int stall_window,
                     int* iters_done, double* device_ms);
