@@ -64,6 +64,23 @@ CASES = {
                                   deck=dict(order=2, flux="roe", gradient="leastsquares", limiter="venkatakrishnan",
                                             k=5.0, omega=OMEGA, mach=0.5, aoa_deg=1.0, stages=4, cfl=1.0),
                                   iters=20, dump_iters=[1, 20]),
+    # the other four flux x gradient x limiter pairings, so all eight are pinned
+    "t3_o2_gg_bj_roe": dict(kind="tet", n=3, blocks=1,
+                            deck=dict(order=2, flux="roe", gradient="greengauss", limiter="barthjespersen",
+                                      omega=OMEGA, mach=0.5, aoa_deg=2.0),
+                            iters=20, dump_iters=[1, 20]),
+    "t4_o2_gg_venk_roe_b2": dict(kind="tet", n=4, blocks=2,
+                                 deck=dict(order=2, flux="roe", gradient="greengauss", limiter="venkatakrishnan",
+                                           k=5.0, omega=OMEGA, mach=0.6, aoa_deg=1.0),
+                                 iters=20, dump_iters=[1, 20]),
+    "t3_o2_ls_bj_ausm": dict(kind="tet", n=3, blocks=1,
+                             deck=dict(order=2, flux="ausm", gradient="leastsquares", limiter="barthjespersen",
+                                       omega=OMEGA, mach=0.6, aoa_deg=3.0),
+                             iters=20, dump_iters=[1, 20]),
+    "t3_o2_ls_venk_ausm": dict(kind="tet", n=3, blocks=1,
+                               deck=dict(order=2, flux="ausm", gradient="leastsquares", limiter="venkatakrishnan",
+                                         k=5.0, omega=OMEGA, mach=0.7, aoa_deg=1.25),
+                               iters=20, dump_iters=[1, 20]),
     "h5_o2_ls_venk_roe": dict(kind="hex", n=5, nz=1,
                               deck=dict(order=2, flux="roe", gradient="leastsquares", limiter="venkatakrishnan",
                                         k=5.0, omega=OMEGA, mach=0.6, aoa_deg=3.0, cfl=0.5),
