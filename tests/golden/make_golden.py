@@ -79,7 +79,7 @@ CASES = {
                              iters=20, dump_iters=[1, 20]),
     "t3_o2_ls_venk_ausm": dict(kind="tet", n=3, blocks=1,
                                deck=dict(order=2, flux="ausm", gradient="leastsquares", limiter="venkatakrishnan",
-                                         k=5.0, omega=OMEGA, mach=0.7, aoa_deg=1.25),
+                                         k=5.0, omega=OMEGA, mach=0.6, aoa_deg=3.0),
                                iters=20, dump_iters=[1, 20]),
     "h5_o2_ls_venk_roe": dict(kind="hex", n=5, nz=1,
                               deck=dict(order=2, flux="roe", gradient="leastsquares", limiter="venkatakrishnan",
