@@ -122,13 +122,19 @@ def fp32_error_report(td):
 
 def workload_config(n, blocks, precision):
     w = WORKLOAD
-    return {"workload": f"bump channel {n}^3 hex x 6 tets ({6 * n ** 3:,} tets), {blocks} slab blocks on one GPU, "
+    cells = 6 * n ** 3
+    # bytes the reconstruction pass must touch per launch: about 16 + 50 b per
+    # tet (states, neighbour ids, least-squares weights, r-vectors, face states)
+    mb = cells * (16 + 50 * (4 if precision == "fp32" else 8)) / 1e6
+    l2 = (f"each stage pass touches about {mb:,.0f} MB, more than the 126 MB L2; no flush needed" if mb > 126
+          else f"each stage pass touches about {mb:,.1f} MB, less than the 126 MB L2: a test size, not a bench number")
+    return {"workload": f"bump channel {n}^3 hex x 6 tets ({cells:,} tets), {blocks} slab blocks on one GPU, "
                         f"{w['gradient']} + {w['limiter']} (K={w['k']:g}) + {w['flux']}, M {w['mach']}, "
                         f"alpha {w['aoa_deg']}, {w['stages']}-stage RK, CFL {w['cfl']}",
-            "cells": 6 * n ** 3, "blocks": blocks,
+            "cells": cells, "blocks": blocks,
             "arithmetic": "fp32 fluxes/gradients/limiters, fp64 conserved state and reductions"
             if precision == "fp32" else "fp64 throughout (reference arithmetic)",
-            "l2": "working set (several GB) far larger than the 126 MB L2; no flush needed"}
+            "l2": l2}
 
 
 # ------------------------------------------------------------------ clocks
