@@ -38,8 +38,14 @@ int main(int argc, char** argv) {
 	for (int i = 2; i < argc; i++) {
 		if (!std::strcmp(argv[i], "--fp32")) opt.precision = E3D_FP32;
 		else if (!std::strcmp(argv[i], "--no-graph")) opt.use_graph = 0;
-		else if (!std::strcmp(argv[i], "--check-every") && i + 1 < argc) check_every = std::atoi(argv[++i]);
-		else {
+		else if (!std::strcmp(argv[i], "--check-every") && i + 1 < argc) {
+			// each pass of the loop below must advance, or the stop test never runs
+			check_every = std::atoi(argv[++i]);
+			if (check_every < 1) {
+				std::cerr << "--check-every needs a positive iteration count" << std::endl;
+				return 2;
+			}
+		} else {
 			std::cerr << "unknown option " << argv[i] << std::endl;
 			return 2;
 		}

@@ -126,11 +126,14 @@ struct Key {
 	}
 	bool operator==(const Key& o) const { return n[0] == o.n[0] && n[1] == o.n[1] && n[2] == o.n[2] && n[3] == o.n[3]; }
 };
+// nn is 3 or 4: face node lists come from the tet/hex face tables and boundary
+// elements are read as triangles or quadrilaterals only
 Key make_key(const int* nodes, int nn) {
 	Key k;
 	k.n[3] = -1;
 	for (int i = 0; i < nn; i++) k.n[i] = nodes[i];
-	std::sort(k.n, k.n + nn);
+	for (int i = 1; i < nn; i++)
+		for (int j = i; j > 0 && k.n[j - 1] > k.n[j]; j--) std::swap(k.n[j - 1], k.n[j]);
 	return k;
 }
 
