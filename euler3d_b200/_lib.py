@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libe3d.so")
 E3D_OK = 0
 ERRORS = {
     -1: "E3D_ERR_ARG", -2: "E3D_ERR_IO", -3: "E3D_ERR_FORMAT", -4: "E3D_ERR_MESH", -5: "E3D_ERR_CUDA",
-    -6: "E3D_ERR_NONFINITE", -7: "E3D_ERR_STATE", -8: "E3D_ERR_TIMEOUT", -9: "E3D_ERR_LIMIT",
+    -6: "E3D_ERR_NONFINITE", -7: "E3D_ERR_STATE", -9: "E3D_ERR_LIMIT",
 }
 GRAD = {"greengauss": 0, "leastsquares": 1}
 LIM = {"barthjespersen": 0, "venkatakrishnan": 1}

@@ -36,7 +36,11 @@ constexpr int kMaxDevices = 64;
 __device__ __align__(256) double g_norm_scratch[E3D_NOALLOC_MAX_PARTIALS * 5];
 
 // partial[(b*max_chunks + chunk)*5 + q] = sum over the chunk's cells of (rc-rd)^2;
-// every slot of the grid is written, so nothing needs clearing between calls
+// every slot of the grid is written, so nothing needs clearing between calls.
+// The grid covers max_chunks * kChunk cells per block.  A block whose offsets
+// span more cells than that (max_block_cells understated by the caller) would
+// lose its tail silently; instead its last chunk writes NaN, so all five of
+// that block's outputs come back NaN.
 __global__ void __launch_bounds__(kThreads) k_partial_static(const double* __restrict__ rc, const double* __restrict__ rd,
                                                              long long n, const int* __restrict__ off, int max_chunks,
                                                              double* __restrict__ partial) {
@@ -45,6 +49,7 @@ __global__ void __launch_bounds__(kThreads) k_partial_static(const double* __res
 	const long long o0 = max(0LL, min((long long)off[b], n)), o1 = max(o0, min((long long)off[b + 1], n));
 	const long long beg = o0 + (long long)blockIdx.x * kChunk;
 	const long long end = min(o1, beg + kChunk);
+	const bool uncovered = blockIdx.x == max_chunks - 1 && o1 - o0 > (long long)max_chunks * kChunk;
 	double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
 	for (long long c = beg + threadIdx.x; c < end; c += kThreads)
 		for (int q = 0; q < 5; q++) {
@@ -59,7 +64,9 @@ __global__ void __launch_bounds__(kThreads) k_partial_static(const double* __res
 			for (int q = 0; q < 5; q++) sm[q][threadIdx.x] += sm[q][threadIdx.x + w];
 		__syncthreads();
 	}
-	if (threadIdx.x < 5) partial[((size_t)b * max_chunks + blockIdx.x) * 5 + threadIdx.x] = sm[threadIdx.x][0];
+	if (threadIdx.x < 5)
+		partial[((size_t)b * max_chunks + blockIdx.x) * 5 + threadIdx.x] = uncovered ? __longlong_as_double(0x7ff8000000000000LL)
+		                                                                             : sm[threadIdx.x][0];
 }
 
 __global__ void k_final_static(const double* __restrict__ partial, int n_blocks, int max_chunks, double* __restrict__ out) {
@@ -109,14 +116,16 @@ extern "C" int e3d_residual_norms_noalloc(const double* rc, const double* rd, in
 		e3d::set_last_error("e3d_residual_norms_noalloc: null pointer or negative size");
 		return E3D_ERR_ARG;
 	}
-	const int max_chunks = max_block_cells > 0 ? (max_block_cells + kChunk - 1) / kChunk : 1;
-	if ((long long)n_blocks * max_chunks > E3D_NOALLOC_MAX_PARTIALS) {
+	// chunk count in 64 bits: a max_block_cells near INT_MAX must not wrap
+	const long long chunks64 = max_block_cells > 0 ? ((long long)max_block_cells + kChunk - 1) / kChunk : 1;
+	if ((long long)n_blocks * chunks64 > E3D_NOALLOC_MAX_PARTIALS) {
 		e3d::set_last_error("e3d_residual_norms_noalloc: " + std::to_string(n_blocks) + " blocks x " +
-		                    std::to_string(max_chunks) + " chunks of " + std::to_string(kChunk) +
+		                    std::to_string(chunks64) + " chunks of " + std::to_string(kChunk) +
 		                    " cells exceed the static scratch of " + std::to_string(E3D_NOALLOC_MAX_PARTIALS) +
 		                    " partial sums");
 		return E3D_ERR_LIMIT;
 	}
+	const int max_chunks = static_cast<int>(chunks64);  // <= E3D_NOALLOC_MAX_PARTIALS here
 	double* scratch = nullptr;
 	const int rcode = scratch_for_current_device(&scratch);
 	if (rcode != E3D_OK) return rcode;

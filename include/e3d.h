@@ -29,7 +29,6 @@ extern "C" {
 #define E3D_ERR_CUDA (-5)      /* CUDA runtime error */
 #define E3D_ERR_NONFINITE (-6) /* a residual norm became NaN or infinite */
 #define E3D_ERR_STATE (-7)     /* call not valid in this solver state / precision */
-#define E3D_ERR_TIMEOUT (-8)   /* a bounded wait expired */
 #define E3D_ERR_LIMIT (-9)     /* size above a documented maximum */
 
 /* strategy selectors: the reference's string choices
@@ -257,6 +256,10 @@ int e3d_state_import(e3d_solver* s, const void* host, int64_t bytes);
  *                  must not exceed E3D_NOALLOC_MAX_PARTIALS (else E3D_ERR_LIMIT)
  *   out            device [n_blocks*5]
  *   stream         cudaStream_t or NULL
+ * The host cannot read the device offsets, so it trusts max_block_cells: a
+ * block with more cells than ceil(max_block_cells/4096)*4096 gets NaN in all
+ * five of its outputs (found on the device; the call still returns E3D_OK),
+ * never a silently truncated sum.
  * Queued on `stream`, nothing is allocated or freed.  The first call on a
  * device looks up the scratch address (cudaGetSymbolAddress): make it before
  * any stream capture.  Calls share the scratch, so calls that overlap on the

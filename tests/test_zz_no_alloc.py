@@ -58,10 +58,15 @@ def _call(t_rc, t_rd, t_off, t_out, n, max_cells):
 def _check_case(solver, case):
     solver.iterate(3)
     ref = solver.flow_data()[:, :5]  # existing entry point: per-block sums of (Rc-Rd)^2
-    args = _residuals_on_device(solver, case)
-    first = _call(*args)
-    second = _call(*args)
+    t_rc, t_rd, t_off, t_out, n, max_cells = _residuals_on_device(solver, case)
+    first = _call(t_rc, t_rd, t_off, t_out, n, max_cells)
+    # a call with a different chunk layout in between: a larger max_block_cells
+    # puts each block's partial sums at other scratch indices, so a second call
+    # with the first layout would read stale partials if any were left unwritten
+    wide = _call(t_rc, t_rd, t_off, t_out, n, max_cells + 3 * 4096)
+    second = _call(t_rc, t_rd, t_off, t_out, n, max_cells)
     assert max_rel(first, ref) <= RTOL
+    assert max_rel(wide, ref) <= RTOL
     assert max_rel(second, ref) <= RTOL
 
 
@@ -78,6 +83,23 @@ def test_noalloc_norms_match_flow_data_several_chunks(tmp_path):
     _check_case(api.Solver(case, precision="fp64", device=0), case)
 
 
+def test_noalloc_understated_block_size_gives_nan(tmp_path):
+    # max_block_cells below the real size: the host cannot see the device
+    # offsets, so the blocks the grid does not cover come back NaN (never a
+    # silently truncated sum); blocks that fit stay exact
+    deck = mg.write_case(str(tmp_path), 16, 4, deck=mg.Deck(topology="", order=2, mach=0.7, aoa_deg=1.25))
+    case = api.Case(deck)
+    solver = api.Solver(case, precision="fp64", device=0)
+    solver.iterate(2)
+    ref = solver.flow_data()[:, :5]
+    t_rc, t_rd, t_off, t_out, n, max_cells = _residuals_on_device(solver, case)
+    assert max_cells > 4096  # every block needs two chunks
+    got = _call(t_rc, t_rd, t_off, t_out, n, 4096)
+    assert np.all(np.isnan(got))
+    again = _call(t_rc, t_rd, t_off, t_out, n, max_cells)
+    assert max_rel(again, ref) <= RTOL
+
+
 def test_noalloc_rejects_sizes_beyond_the_scratch():
     # rejected on the host before anything is launched; no pointer is touched
     nb = 3
@@ -86,3 +108,7 @@ def test_noalloc_rejects_sizes_beyond_the_scratch():
                                             C.c_void_p(16), None)
     assert rc == -9
     assert b"static scratch" in L.lib().e3d_last_error()
+    # a max_block_cells near INT_MAX is rejected too (its chunk count is formed in 64 bits)
+    rc = L.lib().e3d_residual_norms_noalloc(C.c_void_p(16), C.c_void_p(16), 1, 1, C.c_void_p(16), 2**31 - 1,
+                                            C.c_void_p(16), None)
+    assert rc == -9
