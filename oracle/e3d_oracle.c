@@ -1,16 +1,84 @@
 /*
- * e3d_oracle.c -- CPU restatement of the euler3D residual/update path (FP64).
+ * e3d_oracle.c -- CPU restatement of the euler3D residual/update path.
  *
  * TEST INFRASTRUCTURE ONLY (see e3d_oracle.h).  Compiled with
  * -O2 -ffp-contract=off; every expression keeps the reference's operand order
  * (file:line cited per function) so results are bit-identical to the
  * reference's x86-64 build.
+ *
+ * The same source builds a second library, libe3d_oracle32.so
+ * (-DE3D_ORACLE_FP32): a model of the B200 FP32 variant used to derive that
+ * variant's error bounds.  There `real` is float and values are rounded where
+ * the FP32 kernels round them: geometry (unit normals, areas, r-vectors,
+ * least-squares weights, volumes) and primitives are held in FP32; gradient,
+ * limiter, flux, time-step and boundary arithmetic runs in FP32; the residual
+ * accumulators are FP32; the conservative update is FP64 from FP32 residuals,
+ * and the FP64 conservative state W is carried from stage to stage across
+ * iterations (W0 of the next iteration = W of the last stage, starting from
+ * the FP64 freestream state); norms and forces are FP64 sums.  The FP32
+ * Venkatakrishnan limiter uses the kernels' one-division form and the face
+ * value of a tetrahedron's own side is q + phi (g.r).  e3d_oracle_set_noise
+ * moves each face flux by one FP32 unit up or down, or leaves it, by a seeded
+ * hash (what another FP32 evaluation order, contraction or approximate
+ * division gives): independent rounding realisations for the error
+ * distribution.
+ * In the FP64 build (real = double) every macro below is the identity and
+ * the arithmetic is the reference's.
  */
+#include <stdint.h>
 #include <stdlib.h>
 #include "e3d_oracle.h"
 
 #include <math.h>
 #include <string.h>
+
+#ifdef E3D_ORACLE_FP32
+typedef float real;
+#define r_sqrt sqrtf
+#define r_fabs fabsf
+#define r_fmin fminf
+#define r_copysign copysignf
+#define FP32_MODEL 1
+#else
+typedef double real;
+#define r_sqrt sqrt
+#define r_fabs fabs
+#define r_fmin fmin
+#define r_copysign copysign
+#define FP32_MODEL 0
+#endif
+#define K(x) ((real)(x))            /* a constant or a double parameter in working precision */
+#define LD(x) ((real)(x))           /* an array value read in working precision */
+#define ST(x) ((double)(real)(x))   /* a value stored in working precision */
+
+static uint64_t g_noise_seed = 0, g_noise_calls = 0;
+
+void e3d_oracle_set_noise(unsigned long long seed) {
+	g_noise_seed = seed;
+	g_noise_calls = 0;
+}
+
+#if FP32_MODEL
+/* splitmix64 finaliser: fixed pseudo-random bits per (seed, call, face, variable) */
+static uint64_t mix64(uint64_t x) {
+	x += 0x9e3779b97f4a7c15ULL;
+	x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+	x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+	return x ^ (x >> 31);
+}
+/* A face flux as another FP32 evaluation order could give it: unchanged, one
+ * FP32 unit up or one down (seeded hash: 1/2, 1/4, 1/4).  The identity while
+ * no seed is set. */
+static float perturb_flux(float v, int f, int q) {
+	if (!g_noise_seed) return v;
+	const uint64_t h = mix64(g_noise_seed ^ mix64(g_noise_calls * 0x100000001b3ULL + (uint64_t)f * 8u + (uint64_t)q));
+	if (!(h & 1)) return v;
+	return nextafterf(v, (h & 2) ? INFINITY : -INFINITY);
+}
+#define FLUX_OUT(v, f, q) perturb_flux((v), (f), (q))
+#else
+#define FLUX_OUT(v, f, q) (v)
+#endif
 
 #define V5(a, n, q, c) ((a)[(size_t)(q) * (size_t)(n) + (size_t)(c)])
 #define G3(a, n, q, c, d) ((a)[((size_t)(q) * (size_t)(n) + (size_t)(c)) * 3 + (d)])
@@ -34,7 +102,7 @@ void e3d_oracle_init_state(e3d_oracle_block* b, const e3d_oracle_params* p) {
 	double f[5];
 	e3d_oracle_freestream(p, f);
 	for (int q = 0; q < 5; q++)
-		for (int c = 0; c < b->n_all; c++) V5(b->prim, b->n_all, q, c) = f[q];
+		for (int c = 0; c < b->n_all; c++) V5(b->prim, b->n_all, q, c) = ST(f[q]);
 	memset(b->conv_res, 0, sizeof(double) * 5 * (size_t)b->n_all);
 	memset(b->diss_res, 0, sizeof(double) * 5 * (size_t)b->n_all);
 	memset(b->w0, 0, sizeof(double) * 5 * (size_t)b->n_all);
@@ -62,8 +130,8 @@ void e3d_oracle_save_w0(e3d_oracle_block* b, const e3d_oracle_params* p) {
 void e3d_oracle_spectral_radius(e3d_oracle_block* b, const e3d_oracle_params* p) {
 	const int n = b->n_all;
 	for (int c = 0; c < b->n_real; c++) {
-		const double cc = sqrt(p->gamma * V5(b->prim, n, 4, c) / V5(b->prim, n, 0, c));
-		b->spectral_radius[c] = 0.0;
+		const real cc = r_sqrt(K(p->gamma) * LD(V5(b->prim, n, 4, c)) / LD(V5(b->prim, n, 0, c)));
+		real sr = K(0.0);
 		for (int k = b->cell_face_ptr[c]; k < b->cell_face_ptr[c + 1]; k++) {
 			const int f = b->cell_faces[k];
 			double nx = b->face_normal[3 * f], ny = b->face_normal[3 * f + 1], nz = b->face_normal[3 * f + 2];
@@ -71,15 +139,19 @@ void e3d_oracle_spectral_radius(e3d_oracle_block* b, const e3d_oracle_params* p)
 			nx /= ds;
 			ny /= ds;
 			nz /= ds;
-			b->spectral_radius[c] +=
-			    (fabs((V5(b->prim, n, 1, c)) * nx + (V5(b->prim, n, 2, c)) * ny + (V5(b->prim, n, 3, c)) * nz) + (cc)) * ds;
+			sr += (r_fabs((LD(V5(b->prim, n, 1, c))) * K(nx) + (LD(V5(b->prim, n, 2, c))) * K(ny) +
+			              (LD(V5(b->prim, n, 3, c))) * K(nz)) +
+			       (cc)) *
+			      K(ds);
 		}
+		b->spectral_radius[c] = ST(sr);
 	}
 }
 
 /* Timestep::computeTimestep (Timestep.cpp:123-148) */
 void e3d_oracle_timestep(e3d_oracle_block* b, const e3d_oracle_params* p) {
-	for (int c = 0; c < b->n_real; c++) b->dt[c] = p->cfl * b->cell_volume[c] / b->spectral_radius[c];
+	for (int c = 0; c < b->n_real; c++)
+		b->dt[c] = ST(K(p->cfl) * LD(b->cell_volume[c]) / LD(b->spectral_radius[c]));
 }
 
 /* Ghost-gradient reflection about the face plane for the ghosts of the first
@@ -94,15 +166,17 @@ static void reflect_ghost_gradients(e3d_oracle_block* b) {
 				const int f = b->cell_faces[b->cell_face_ptr[ext]];
 				const int in = b->face_cells[2 * f];
 				const double area = b->face_area[f];
-				double nn[3];
+				real nn[3];
 				for (int d = 0; d < 3; d++) {
-					nn[d] = b->face_normal[3 * f + d];
-					nn[d] /= area;
+					double t = b->face_normal[3 * f + d];
+					t /= area;
+					nn[d] = K(t);
 				}
 				for (int q = 0; q < 5; q++) {
-					double dot = 0.0;
-					for (int d = 0; d < 3; d++) dot += G3(b->grad, n, q, in, d) * nn[d];
-					for (int d = 0; d < 3; d++) G3(b->grad, n, q, ext, d) = G3(b->grad, n, q, in, d) - 2.0 * dot * nn[d];
+					real dot = K(0.0);
+					for (int d = 0; d < 3; d++) dot += LD(G3(b->grad, n, q, in, d)) * nn[d];
+					for (int d = 0; d < 3; d++)
+						G3(b->grad, n, q, ext, d) = ST(LD(G3(b->grad, n, q, in, d)) - K(2.0) * dot * nn[d]);
 				}
 			}
 		}
@@ -116,6 +190,8 @@ void e3d_oracle_gradients(e3d_oracle_block* b, int kind) {
 	const int n = b->n_all;
 	memset(b->grad, 0, sizeof(double) * 15 * (size_t)n);
 	for (int c = 0; c < b->n_real; c++) {
+		real acc[5][3];
+		for (int q = 0; q < 5; q++) acc[q][0] = acc[q][1] = acc[q][2] = K(0.0);
 		for (int k = b->cell_face_ptr[c]; k < b->cell_face_ptr[c + 1]; k++) {
 			if (kind == 0) {
 				const int f = b->cell_faces[k];
@@ -125,18 +201,20 @@ void e3d_oracle_gradients(e3d_oracle_block* b, int kind) {
 				const int l = b->face_cells[2 * f], r = b->face_cells[2 * f + 1];
 				for (int d = 0; d < 3; d++)
 					for (int q = 0; q < 5; q++)
-						G3(b->grad, n, q, c, d) += 0.5 * (V5(b->prim, n, q, l) + V5(b->prim, n, q, r)) * nn[d];
+						acc[q][d] += K(0.5) * (LD(V5(b->prim, n, q, l)) + LD(V5(b->prim, n, q, r))) * K(nn[d]);
 			} else {
 				const int nb = b->cell_cells[k];
 				const double* w = &b->ls_weights[3 * (size_t)k];
 				for (int d = 0; d < 3; d++)
 					for (int q = 0; q < 5; q++)
-						G3(b->grad, n, q, c, d) += w[d] * (V5(b->prim, n, q, nb) - V5(b->prim, n, q, c));
+						acc[q][d] += LD(w[d]) * (LD(V5(b->prim, n, q, nb)) - LD(V5(b->prim, n, q, c)));
 			}
 		}
 		if (kind == 0)
 			for (int d = 0; d < 3; d++)
-				for (int q = 0; q < 5; q++) G3(b->grad, n, q, c, d) /= b->cell_volume[c];
+				for (int q = 0; q < 5; q++) acc[q][d] /= LD(b->cell_volume[c]);
+		for (int q = 0; q < 5; q++)
+			for (int d = 0; d < 3; d++) G3(b->grad, n, q, c, d) = ST(acc[q][d]);
 	}
 	reflect_ghost_gradients(b);
 }
@@ -146,34 +224,43 @@ void e3d_oracle_gradients(e3d_oracle_block* b, int kind) {
 void e3d_oracle_limiters(e3d_oracle_block* b, int kind, double omega, double k) {
 	const int n = b->n_all;
 	for (int c = 0; c < n; c++) {
-		const double eps2 = k * k * k * (b->cell_volume[c]);
-		double mx[5], mn[5], dmax[5], dmin[5];
-		for (int q = 0; q < 5; q++) mx[q] = mn[q] = V5(b->prim, n, q, c);
+		const real eps2 = K(k * k * k) * LD(b->cell_volume[c]);
+		real mx[5], mn[5], dmax[5], dmin[5], phi[5];
+		for (int q = 0; q < 5; q++) mx[q] = mn[q] = LD(V5(b->prim, n, q, c));
 		for (int s = b->cell_face_ptr[c]; s < b->cell_face_ptr[c + 1]; s++) {
 			const int nb = b->cell_cells[s];
 			for (int q = 0; q < 5; q++) {
-				const double v = V5(b->prim, n, q, nb);
+				const real v = LD(V5(b->prim, n, q, nb));
 				if (v > mx[q]) mx[q] = v;
 				if (v < mn[q]) mn[q] = v;
 			}
 		}
 		for (int q = 0; q < 5; q++) {
-			dmax[q] = mx[q] - V5(b->prim, n, q, c);
-			dmin[q] = mn[q] - V5(b->prim, n, q, c);
-			V5(b->limiter, n, q, c) = INFINITY;
+			dmax[q] = mx[q] - LD(V5(b->prim, n, q, c));
+			dmin[q] = mn[q] - LD(V5(b->prim, n, q, c));
+			phi[q] = (real)INFINITY;
 		}
 		for (int s = b->cell_face_ptr[c]; s < b->cell_face_ptr[c + 1]; s++) {
 			const int f = b->cell_faces[s];
 			const double* r = (c == b->face_cells[2 * f]) ? &b->r_left[3 * f] : &b->r_right[3 * f];
 			for (int q = 0; q < 5; q++) {
-				double d2 = 0.0, lf;
-				for (int d = 0; d < 3; d++) d2 += G3(b->grad, n, q, c, d) * r[d];
+				real d2 = K(0.0), lf;
+				for (int d = 0; d < 3; d++) d2 += LD(G3(b->grad, n, q, c, d)) * LD(r[d]);
 				if (kind == 0) {
-					d2 = (copysign(1.0, d2)) * (fabs(d2) + omega);
-					if (d2 > 0.0) lf = fmin(1.0, dmax[q] / d2);
-					else if (d2 < 0.0) lf = fmin(1.0, dmin[q] / d2);
-					else lf = 1.0;
+					d2 = (r_copysign(K(1.0), d2)) * (r_fabs(d2) + K(omega));
+					if (d2 > K(0.0)) lf = r_fmin(K(1.0), dmax[q] / d2);
+					else if (d2 < K(0.0)) lf = r_fmin(K(1.0), dmin[q] / d2);
+					else lf = K(1.0);
 				} else {
+#if FP32_MODEL
+					/* the FP32 kernels' form: d2 cancelled, one division */
+					if (!(d2 > 0.0f) && !(d2 < 0.0f)) lf = 1.0f;
+					else {
+						const float D = d2 > 0.0f ? dmax[q] : dmin[q];
+						const float A = fmaf(D, D, eps2);
+						lf = fmaf(2.0f * d2, D, A) / fmaf(d2, fmaf(2.0f, d2, D), A);
+					}
+#else
 					if (d2 > 0.0)
 						lf = (1.0 / d2) * ((dmax[q] * dmax[q] + eps2) * d2 + 2.0 * d2 * d2 * dmax[q]) /
 						     (dmax[q] * dmax[q] + 2.0 * d2 * d2 + dmax[q] * d2 + eps2);
@@ -181,173 +268,219 @@ void e3d_oracle_limiters(e3d_oracle_block* b, int kind, double omega, double k) 
 						lf = (1.0 / d2) * ((dmin[q] * dmin[q] + eps2) * d2 + 2.0 * d2 * d2 * dmin[q]) /
 						     (dmin[q] * dmin[q] + 2.0 * d2 * d2 + dmin[q] * d2 + eps2);
 					else lf = 1.0;
+#endif
 				}
-				if (lf < V5(b->limiter, n, q, c)) V5(b->limiter, n, q, c) = lf;
+				if (lf < phi[q]) phi[q] = lf;
 			}
 		}
+		for (int q = 0; q < 5; q++) V5(b->limiter, n, q, c) = ST(phi[q]);
 	}
 }
 
-/* MUSCL face values of one side (FluxScheme.cpp:127-159) */
-static void side_state(const e3d_oracle_block* b, int c, const double* r, double q[5]) {
+/* 1 when every real cell of the block is a tetrahedron (the FP32 kernels' 4-slot path) */
+static int all_tets(const e3d_oracle_block* b) {
+	for (int c = 0; c < b->n_real; c++)
+		if (b->cell_face_ptr[c + 1] - b->cell_face_ptr[c] != 4) return 0;
+	return 1;
+}
+
+/* MUSCL face values of one side (FluxScheme.cpp:127-159).  FP32 model: a real
+ * tetrahedron's own side is q + phi (g.r), the FP32 kernels' form. */
+static void side_state(const e3d_oracle_block* b, int c, const double* r, real q[5], int tet) {
 	const int n = b->n_all;
+	(void)tet;
 	for (int v = 0; v < 5; v++) {
-		q[v] = V5(b->prim, n, v, c);
-		for (int d = 0; d < 3; d++) q[v] += V5(b->limiter, n, v, c) * G3(b->grad, n, v, c, d) * r[d];
+		q[v] = LD(V5(b->prim, n, v, c));
+#if FP32_MODEL
+		if (tet && c < b->n_real) {
+			real d2 = LD(G3(b->grad, n, v, c, 0)) * LD(r[0]);
+			d2 += LD(G3(b->grad, n, v, c, 1)) * LD(r[1]);
+			d2 += LD(G3(b->grad, n, v, c, 2)) * LD(r[2]);
+			q[v] = q[v] + LD(V5(b->limiter, n, v, c)) * d2;
+			continue;
+		}
+#endif
+		for (int d = 0; d < 3; d++) q[v] += LD(V5(b->limiter, n, v, c)) * LD(G3(b->grad, n, v, c, d)) * LD(r[d]);
 	}
 }
 
-static void face_geometry(const e3d_oracle_block* b, int f, double* nx, double* ny, double* nz, double* nn) {
-	*nx = b->face_normal[3 * f];
-	*ny = b->face_normal[3 * f + 1];
-	*nz = b->face_normal[3 * f + 2];
-	*nn = sqrt(*nx * *nx + *ny * *ny + *nz * *nz);
-	*nx /= *nn;
-	*ny /= *nn;
-	*nz /= *nn;
+/* unit normal and area: the reference's per-face normalisation in FP64 (the
+ * FP32 kernels read these values precomputed and rounded) */
+static void face_geometry(const e3d_oracle_block* b, int f, real* rx, real* ry, real* rz, real* rn) {
+	double nx = b->face_normal[3 * f];
+	double ny = b->face_normal[3 * f + 1];
+	double nz = b->face_normal[3 * f + 2];
+	const double nn = sqrt(nx * nx + ny * ny + nz * nz);
+	nx /= nn;
+	ny /= nn;
+	nz /= nn;
+	*rx = K(nx);
+	*ry = K(ny);
+	*rz = K(nz);
+	*rn = K(nn);
 }
 
 /* FluxScheme::computeFluxConv (Solver/src/FluxScheme.cpp:16-211) for Roe and
  * AusmScheme::computeFluxConv (Solver/src/AusmScheme.cpp:647-871) for AUSM */
 void e3d_oracle_flux_conv(e3d_oracle_block* b, const e3d_oracle_params* p) {
 	const int n = b->n_all;
-	const double g = p->gamma;
+	const real g = K(p->gamma);
+	const real gr = K(p->gamma / (p->gamma - 1.0)); /* g / (g - 1.0), formed in FP64 */
+	const int tet = all_tets(b);
 	for (int c = 0; c < b->n_real; c++)
 		for (int q = 0; q < 5; q++) V5(b->conv_res, n, q, c) = 0.0;
 	for (int f = 0; f < b->n_faces; f++) {
-		double nx, ny, nz, nn, L[5], R[5], fl[5];
+		real nx, ny, nz, nn, L[5], R[5], fl[5];
 		face_geometry(b, f, &nx, &ny, &nz, &nn);
 		const int l = b->face_cells[2 * f], r = b->face_cells[2 * f + 1];
-		side_state(b, l, &b->r_left[3 * f], L);
-		side_state(b, r, &b->r_right[3 * f], R);
-		const double qqL = L[1] * L[1] + L[2] * L[2] + L[3] * L[3];
-		const double HL = (0.5 * qqL + g / (g - 1.0) * L[4] / L[0]);
-		const double VL = L[1] * nx + L[2] * ny + L[3] * nz;
-		const double qqR = R[1] * R[1] + R[2] * R[2] + R[3] * R[3];
-		const double HR = (0.5 * qqR + g / (g - 1.0) * R[4] / R[0]);
-		const double VR = R[1] * nx + R[2] * ny + R[3] * nz;
+		side_state(b, l, &b->r_left[3 * f], L, tet);
+		side_state(b, r, &b->r_right[3 * f], R, tet);
+		const real qqL = L[1] * L[1] + L[2] * L[2] + L[3] * L[3];
+		const real HL = (K(0.5) * qqL + gr * L[4] / L[0]);
+		const real VL = L[1] * nx + L[2] * ny + L[3] * nz;
+		const real qqR = R[1] * R[1] + R[2] * R[2] + R[3] * R[3];
+		const real HR = (K(0.5) * qqR + gr * R[4] / R[0]);
+		const real VR = R[1] * nx + R[2] * ny + R[3] * nz;
 		if (p->flux == 0) {
-			const double FL[5] = {L[0] * VL, L[0] * L[1] * VL + nx * L[4], L[0] * L[2] * VL + ny * L[4],
-			                      L[0] * L[3] * VL + nz * L[4], L[0] * HL * VL};
-			const double FR[5] = {R[0] * VR, R[0] * R[1] * VR + nx * R[4], R[0] * R[2] * VR + ny * R[4],
-			                      R[0] * R[3] * VR + nz * R[4], R[0] * HR * VR};
-			for (int q = 0; q < 5; q++) fl[q] = 0.5 * (FL[q] + FR[q]) * nn;
+			const real FL[5] = {L[0] * VL, L[0] * L[1] * VL + nx * L[4], L[0] * L[2] * VL + ny * L[4],
+			                    L[0] * L[3] * VL + nz * L[4], L[0] * HL * VL};
+			const real FR[5] = {R[0] * VR, R[0] * R[1] * VR + nx * R[4], R[0] * R[2] * VR + ny * R[4],
+			                    R[0] * R[3] * VR + nz * R[4], R[0] * HR * VR};
+			for (int q = 0; q < 5; q++) fl[q] = K(0.5) * (FL[q] + FR[q]) * nn;
 		} else {
-			const double cL = sqrt(g * L[4] / L[0]), ML = VL / cL;
-			double pLp, MLp, pRm, MRm;
-			if (ML <= -1.0) { pLp = 0; MLp = 0; }
-			else if (ML < 1.0) { pLp = L[4] * 0.25 * (ML + 1.0) * (ML + 1.0) * (2.0 - ML); MLp = 0.25 * (ML + 1.0) * (ML + 1.0); }
+			const real cL = r_sqrt(g * L[4] / L[0]), ML = VL / cL;
+			real pLp, MLp, pRm, MRm;
+			if (ML <= K(-1.0)) { pLp = 0; MLp = 0; }
+			else if (ML < K(1.0)) { pLp = L[4] * K(0.25) * (ML + K(1.0)) * (ML + K(1.0)) * (K(2.0) - ML); MLp = K(0.25) * (ML + K(1.0)) * (ML + K(1.0)); }
 			else { MLp = ML; pLp = L[4]; }
-			const double cR = sqrt(g * R[4] / R[0]), MR = VR / cR;
-			if (MR <= -1.0) { pRm = R[4]; MRm = MR; }
-			else if (MR < 1.0) { pRm = R[4] * 0.25 * (1.0 - MR) * (1.0 - MR) * (2.0 + MR); MRm = -0.25 * (MR - 1.0) * (MR - 1.0); }
+			const real cR = r_sqrt(g * R[4] / R[0]), MR = VR / cR;
+			if (MR <= K(-1.0)) { pRm = R[4]; MRm = MR; }
+			else if (MR < K(1.0)) { pRm = R[4] * K(0.25) * (K(1.0) - MR) * (K(1.0) - MR) * (K(2.0) + MR); MRm = K(-0.25) * (MR - K(1.0)) * (MR - K(1.0)); }
 			else { pRm = 0; MRm = 0; }
-			const double M = MLp + MRm;
-			const double FL[5] = {L[0] * cL, L[0] * L[1] * cL, L[0] * L[2] * cL, L[0] * L[3] * cL, L[0] * HL * cL};
-			const double FR[5] = {R[0] * cR, R[0] * R[1] * cR, R[0] * R[2] * cR, R[0] * R[3] * cR, R[0] * HR * cR};
-			fl[0] = 0.5 * M * (FL[0] + FR[0]) * nn;
-			fl[1] = 0.5 * M * (FL[1] + FR[1]) * nn + nx * (pLp + pRm) * nn;
-			fl[2] = 0.5 * M * (FL[2] + FR[2]) * nn + ny * (pLp + pRm) * nn;
-			fl[3] = 0.5 * M * (FL[3] + FR[3]) * nn + nz * (pLp + pRm) * nn;
-			fl[4] = 0.5 * M * (FL[4] + FR[4]) * nn;
+			const real M = MLp + MRm;
+			const real FL[5] = {L[0] * cL, L[0] * L[1] * cL, L[0] * L[2] * cL, L[0] * L[3] * cL, L[0] * HL * cL};
+			const real FR[5] = {R[0] * cR, R[0] * R[1] * cR, R[0] * R[2] * cR, R[0] * R[3] * cR, R[0] * HR * cR};
+			fl[0] = K(0.5) * M * (FL[0] + FR[0]) * nn;
+			fl[1] = K(0.5) * M * (FL[1] + FR[1]) * nn + nx * (pLp + pRm) * nn;
+			fl[2] = K(0.5) * M * (FL[2] + FR[2]) * nn + ny * (pLp + pRm) * nn;
+			fl[3] = K(0.5) * M * (FL[3] + FR[3]) * nn + nz * (pLp + pRm) * nn;
+			fl[4] = K(0.5) * M * (FL[4] + FR[4]) * nn;
 		}
-		for (int q = 0; q < 5; q++) V5(b->conv_res, n, q, l) += fl[q];
-		for (int q = 0; q < 5; q++) V5(b->conv_res, n, q, r) -= fl[q];
+		for (int q = 0; q < 5; q++) fl[q] = FLUX_OUT(fl[q], f, q);
+		for (int q = 0; q < 5; q++) V5(b->conv_res, n, q, l) = ST(LD(V5(b->conv_res, n, q, l)) + fl[q]);
+		for (int q = 0; q < 5; q++) V5(b->conv_res, n, q, r) = ST(LD(V5(b->conv_res, n, q, r)) - fl[q]);
 	}
+	g_noise_calls++;
 }
 
 /* RoeScheme::computeFluxDiss (Solver/src/RoeScheme.cpp:12-311) and
  * AusmScheme::computeFluxDiss (Solver/src/AusmScheme.cpp:12-243) */
 void e3d_oracle_flux_diss(e3d_oracle_block* b, const e3d_oracle_params* p, double beta) {
 	const int n = b->n_all;
-	const double g = p->gamma;
+	const real g = K(p->gamma);
+	const real gr = K(p->gamma / (p->gamma - 1.0)); /* g / (g - 1.0), formed in FP64 */
+	const real gm1 = K(p->gamma - 1.);
+	const real rb = K(beta);
+	const int tet = all_tets(b);
 	for (int c = 0; c < b->n_real; c++)
-		for (int q = 0; q < 5; q++) V5(b->diss_res, n, q, c) *= (1.0 - beta);
+		for (int q = 0; q < 5; q++) V5(b->diss_res, n, q, c) = ST(LD(V5(b->diss_res, n, q, c)) * (K(1.0) - rb));
 	for (int f = 0; f < b->n_faces; f++) {
-		double nx, ny, nz, nn, L[5], R[5], fl[5];
+		real nx, ny, nz, nn, L[5], R[5], fl[5];
 		face_geometry(b, f, &nx, &ny, &nz, &nn);
 		const int l = b->face_cells[2 * f], r = b->face_cells[2 * f + 1];
-		side_state(b, l, &b->r_left[3 * f], L);
-		side_state(b, r, &b->r_right[3 * f], R);
-		const double qqL = L[1] * L[1] + L[2] * L[2] + L[3] * L[3];
-		const double HL = (0.5 * qqL + g / (g - 1.0) * L[4] / L[0]);
-		const double VL = L[1] * nx + L[2] * ny + L[3] * nz;
-		const double qqR = R[1] * R[1] + R[2] * R[2] + R[3] * R[3];
-		const double HR = (0.5 * qqR + g / (g - 1.0) * R[4] / R[0]);
-		const double VR = R[1] * nx + R[2] * ny + R[3] * nz;
+		side_state(b, l, &b->r_left[3 * f], L, tet);
+		side_state(b, r, &b->r_right[3 * f], R, tet);
+		const real qqL = L[1] * L[1] + L[2] * L[2] + L[3] * L[3];
+		const real HL = (K(0.5) * qqL + gr * L[4] / L[0]);
+		const real VL = L[1] * nx + L[2] * ny + L[3] * nz;
+		const real qqR = R[1] * R[1] + R[2] * R[2] + R[3] * R[3];
+		const real HR = (K(0.5) * qqR + gr * R[4] / R[0]);
+		const real VR = R[1] * nx + R[2] * ny + R[3] * nz;
 		if (p->flux == 0) {
-			const double dp = (R[4] - L[4]), dV = (VR - VL), drho = (R[0] - L[0]);
-			const double du = (R[1] - L[1]), dv = (R[2] - L[2]), dw = (R[3] - L[3]);
-			const double rw = sqrt(L[0] * R[0]);
-			const double uw = (L[1] * sqrt(L[0]) + R[1] * sqrt(R[0])) / (sqrt(L[0]) + sqrt(R[0]));
-			const double vw = (L[2] * sqrt(L[0]) + R[2] * sqrt(R[0])) / (sqrt(L[0]) + sqrt(R[0]));
-			const double ww = (L[3] * sqrt(L[0]) + R[3] * sqrt(R[0])) / (sqrt(L[0]) + sqrt(R[0]));
-			const double Hw = (HL * sqrt(L[0]) + HR * sqrt(R[0])) / (sqrt(L[0]) + sqrt(R[0]));
-			const double q2 = uw * uw + vw * vw + ww * ww;
-			const double cw = sqrt((g - 1.) * (Hw - q2 / 2.));
-			const double Vw = uw * nx + vw * ny + ww * nz;
-			const double delta = 1. / 10. * cw;
-			double L1, L234, L5;
-			if (fabs(Vw - cw) <= delta) L1 = (fabs(Vw - cw) * fabs(Vw - cw) + delta * delta) / (2. * delta);
-			else L1 = fabs(Vw - cw);
-			if (fabs(Vw) <= delta) L234 = (fabs(Vw) * fabs(Vw) + delta * delta) / (2. * delta);
-			else L234 = fabs(Vw);
-			if (fabs(Vw + cw) <= delta) L5 = (fabs(Vw + cw) * fabs(Vw + cw) + delta * delta) / (2. * delta);
-			else L5 = fabs(Vw + cw);
-			const double F1 = L1 * (dp - rw * cw * dV) / (2. * cw * cw);
-			const double F234 = (drho - dp / (cw * cw));
-			const double F5 = L5 * (dp + rw * cw * dV) / (2. * cw * cw);
-			const double A0 = F1 * 1. + L234 * (F234 * 1. + rw * 0.) + F5 * 1.;
-			const double A1 = F1 * (uw - cw * nx) + L234 * ((F234 * uw) + rw * (du - dV * nx)) + F5 * (uw + cw * nx);
-			const double A2 = F1 * (vw - cw * ny) + L234 * ((F234 * vw) + rw * (dv - dV * ny)) + F5 * (vw + cw * ny);
-			const double A3 = F1 * (ww - cw * nz) + L234 * ((F234 * ww) + rw * (dw - dV * nz)) + F5 * (ww + cw * nz);
-			const double A4 = F1 * (Hw - cw * Vw) +
-			                  L234 * ((F234 * q2 / 2.) + rw * (uw * du + vw * dv + ww * dw - Vw * dV)) +
-			                  F5 * (Hw + cw * Vw);
-			fl[0] = 0.5 * (A0)*nn;
-			fl[1] = 0.5 * (A1)*nn;
-			fl[2] = 0.5 * (A2)*nn;
-			fl[3] = 0.5 * (A3)*nn;
-			fl[4] = 0.5 * (A4)*nn;
+			const real dp = (R[4] - L[4]), dV = (VR - VL), drho = (R[0] - L[0]);
+			const real du = (R[1] - L[1]), dv = (R[2] - L[2]), dw = (R[3] - L[3]);
+			const real rw = r_sqrt(L[0] * R[0]);
+			const real uw = (L[1] * r_sqrt(L[0]) + R[1] * r_sqrt(R[0])) / (r_sqrt(L[0]) + r_sqrt(R[0]));
+			const real vw = (L[2] * r_sqrt(L[0]) + R[2] * r_sqrt(R[0])) / (r_sqrt(L[0]) + r_sqrt(R[0]));
+			const real ww = (L[3] * r_sqrt(L[0]) + R[3] * r_sqrt(R[0])) / (r_sqrt(L[0]) + r_sqrt(R[0]));
+			const real Hw = (HL * r_sqrt(L[0]) + HR * r_sqrt(R[0])) / (r_sqrt(L[0]) + r_sqrt(R[0]));
+			const real q2 = uw * uw + vw * vw + ww * ww;
+			const real cw = r_sqrt(gm1 * (Hw - q2 / K(2.)));
+			const real Vw = uw * nx + vw * ny + ww * nz;
+			const real delta = K(1. / 10.) * cw;
+			real L1, L234, L5;
+			if (r_fabs(Vw - cw) <= delta) L1 = (r_fabs(Vw - cw) * r_fabs(Vw - cw) + delta * delta) / (K(2.) * delta);
+			else L1 = r_fabs(Vw - cw);
+			if (r_fabs(Vw) <= delta) L234 = (r_fabs(Vw) * r_fabs(Vw) + delta * delta) / (K(2.) * delta);
+			else L234 = r_fabs(Vw);
+			if (r_fabs(Vw + cw) <= delta) L5 = (r_fabs(Vw + cw) * r_fabs(Vw + cw) + delta * delta) / (K(2.) * delta);
+			else L5 = r_fabs(Vw + cw);
+			const real F1 = L1 * (dp - rw * cw * dV) / (K(2.) * cw * cw);
+			const real F234 = (drho - dp / (cw * cw));
+			const real F5 = L5 * (dp + rw * cw * dV) / (K(2.) * cw * cw);
+			const real A0 = F1 * K(1.) + L234 * (F234 * K(1.) + rw * K(0.)) + F5 * K(1.);
+			const real A1 = F1 * (uw - cw * nx) + L234 * ((F234 * uw) + rw * (du - dV * nx)) + F5 * (uw + cw * nx);
+			const real A2 = F1 * (vw - cw * ny) + L234 * ((F234 * vw) + rw * (dv - dV * ny)) + F5 * (vw + cw * ny);
+			const real A3 = F1 * (ww - cw * nz) + L234 * ((F234 * ww) + rw * (dw - dV * nz)) + F5 * (ww + cw * nz);
+			const real A4 = F1 * (Hw - cw * Vw) +
+			                L234 * ((F234 * q2 / K(2.)) + rw * (uw * du + vw * dv + ww * dw - Vw * dV)) +
+			                F5 * (Hw + cw * Vw);
+			fl[0] = K(0.5) * (A0)*nn;
+			fl[1] = K(0.5) * (A1)*nn;
+			fl[2] = K(0.5) * (A2)*nn;
+			fl[3] = K(0.5) * (A3)*nn;
+			fl[4] = K(0.5) * (A4)*nn;
 		} else {
-			const double delta = 0.25;
-			const double cL = sqrt(g * L[4] / L[0]), ML = VL / cL;
-			double MLp, MRm;
-			if (ML <= -1.0) MLp = 0;
-			else if (ML < 1.0) MLp = 0.25 * (ML + 1.0) * (ML + 1.0);
+			const real delta = K(0.25);
+			const real cL = r_sqrt(g * L[4] / L[0]), ML = VL / cL;
+			real MLp, MRm;
+			if (ML <= K(-1.0)) MLp = 0;
+			else if (ML < K(1.0)) MLp = K(0.25) * (ML + K(1.0)) * (ML + K(1.0));
 			else MLp = ML;
-			const double cR = sqrt(g * R[4] / R[0]), MR = VR / cR;
-			if (MR <= -1.0) MRm = MR;
-			else if (MR < 1.0) MRm = -0.25 * (MR - 1.0) * (MR - 1.0);
+			const real cR = r_sqrt(g * R[4] / R[0]), MR = VR / cR;
+			if (MR <= K(-1.0)) MRm = MR;
+			else if (MR < K(1.0)) MRm = K(-0.25) * (MR - K(1.0)) * (MR - K(1.0));
 			else MRm = 0;
-			double M = MLp + MRm;
-			if (fabs(M) > delta) {
+			real M = MLp + MRm;
+			if (r_fabs(M) > delta) {
 			} else {
-				M = (M * M + delta * delta) / (2.0 * delta);
+				M = (M * M + delta * delta) / (K(2.0) * delta);
 			}
-			const double FL[5] = {L[0] * cL, L[0] * L[1] * cL, L[0] * L[2] * cL, L[0] * L[3] * cL, L[0] * HL * cL};
-			const double FR[5] = {R[0] * cR, R[0] * R[1] * cR, R[0] * R[2] * cR, R[0] * R[3] * cR, R[0] * HR * cR};
-			for (int q = 0; q < 5; q++) fl[q] = 0.5 * fabs(M) * (-FL[q] + FR[q]) * nn;
+			const real FL[5] = {L[0] * cL, L[0] * L[1] * cL, L[0] * L[2] * cL, L[0] * L[3] * cL, L[0] * HL * cL};
+			const real FR[5] = {R[0] * cR, R[0] * R[1] * cR, R[0] * R[2] * cR, R[0] * R[3] * cR, R[0] * HR * cR};
+			for (int q = 0; q < 5; q++) fl[q] = K(0.5) * r_fabs(M) * (-FL[q] + FR[q]) * nn;
 		}
-		for (int q = 0; q < 5; q++) V5(b->diss_res, n, q, l) += fl[q] * beta;
-		for (int q = 0; q < 5; q++) V5(b->diss_res, n, q, r) -= fl[q] * beta;
+		for (int q = 0; q < 5; q++) fl[q] = FLUX_OUT(fl[q], f, q);
+		for (int q = 0; q < 5; q++) V5(b->diss_res, n, q, l) = ST(LD(V5(b->diss_res, n, q, l)) + fl[q] * rb);
+		for (int q = 0; q < 5; q++) V5(b->diss_res, n, q, r) = ST(LD(V5(b->diss_res, n, q, r)) - fl[q] * rb);
 	}
+	g_noise_calls++;
 }
 
-/* Updater::updateInternalBlock (Solver/src/Updater.cpp:12-78) */
-void e3d_oracle_update_internal(e3d_oracle_block* b, const e3d_oracle_params* p, double alpha) {
+/* Updater::updateInternalBlock (Solver/src/Updater.cpp:12-78).  FP32 model:
+ * the coefficient alpha dt / V and the residual difference in FP32, the update
+ * and the primitive recovery in FP64, primitives stored in FP32; wout (when
+ * set) receives the FP64 conservative state. */
+static void update_internal(e3d_oracle_block* b, const e3d_oracle_params* p, double alpha, double* wout) {
 	const int n = b->n_all;
+	const double gm1 = (double)K(p->gamma - 1.0);
 	for (int c = 0; c < b->n_real; c++) {
 		double w[5];
 		for (int q = 0; q < 5; q++)
-			w[q] = V5(b->w0, n, q, c) -
-			       (alpha * b->dt[c] / b->cell_volume[c]) * (V5(b->conv_res, n, q, c) - V5(b->diss_res, n, q, c));
-		V5(b->prim, n, 0, c) = w[0];
-		V5(b->prim, n, 1, c) = w[1] / w[0];
-		V5(b->prim, n, 2, c) = w[2] / w[0];
-		V5(b->prim, n, 3, c) = w[3] / w[0];
-		V5(b->prim, n, 4, c) = (p->gamma - 1.0) * (w[4] - 0.5 * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]) / w[0]);
+			w[q] = V5(b->w0, n, q, c) - (double)(K(alpha) * LD(b->dt[c]) / LD(b->cell_volume[c])) *
+			                                (double)(LD(V5(b->conv_res, n, q, c)) - LD(V5(b->diss_res, n, q, c)));
+		V5(b->prim, n, 0, c) = ST(w[0]);
+		V5(b->prim, n, 1, c) = ST(w[1] / w[0]);
+		V5(b->prim, n, 2, c) = ST(w[2] / w[0]);
+		V5(b->prim, n, 3, c) = ST(w[3] / w[0]);
+		V5(b->prim, n, 4, c) = ST(gm1 * (w[4] - 0.5 * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]) / w[0]));
+		if (wout)
+			for (int q = 0; q < 5; q++) wout[(size_t)q * n + c] = w[q];
 	}
+}
+
+void e3d_oracle_update_internal(e3d_oracle_block* b, const e3d_oracle_params* p, double alpha) {
+	update_internal(b, p, alpha, 0);
 }
 
 /* Updater::updateBoundary (Updater.cpp:80-88): WallCellIds / SymmetryCellIds
@@ -395,8 +528,10 @@ void e3d_oracle_smooth(e3d_oracle_block* b) {
 
 void e3d_oracle_update_boundary(e3d_oracle_block* b, const e3d_oracle_params* p) {
 	const int n = b->n_all;
-	double fr[5];
-	e3d_oracle_freestream(p, fr);
+	double frd[5];
+	real fr[5];
+	e3d_oracle_freestream(p, frd);
+	for (int q = 0; q < 5; q++) fr[q] = K(frd[q]);
 	int off = 0;
 	for (int j = 0; j < b->n_markers; j++) {
 		const int kind = b->marker_kind[j];
@@ -406,31 +541,32 @@ void e3d_oracle_update_boundary(e3d_oracle_block* b, const e3d_oracle_params* p)
 				const int f = b->cell_faces[b->cell_face_ptr[ext]];
 				const int in = b->cell_cells[b->cell_face_ptr[ext]];
 				const double area = b->face_area[f];
-				double nx = b->face_normal[3 * f], ny = b->face_normal[3 * f + 1], nz = b->face_normal[3 * f + 2];
-				nx /= area;
-				ny /= area;
-				nz /= area;
-				const double ro = V5(b->prim, n, 0, in), uu = V5(b->prim, n, 1, in), vv = V5(b->prim, n, 2, in),
-				             ww = V5(b->prim, n, 3, in), pp = V5(b->prim, n, 4, in);
-				double o[5];
+				double dx = b->face_normal[3 * f], dy = b->face_normal[3 * f + 1], dz = b->face_normal[3 * f + 2];
+				dx /= area;
+				dy /= area;
+				dz /= area;
+				const real nx = K(dx), ny = K(dy), nz = K(dz);
+				const real ro = LD(V5(b->prim, n, 0, in)), uu = LD(V5(b->prim, n, 1, in)), vv = LD(V5(b->prim, n, 2, in)),
+				           ww = LD(V5(b->prim, n, 3, in)), pp = LD(V5(b->prim, n, 4, in));
+				real o[5];
 				if (kind == 1 || kind == 3) {
-					const double un = uu * nx + vv * ny + ww * nz;
-					const double ub = uu - un * nx, vb = vv - un * ny, wb = ww - un * nz;
+					const real un = uu * nx + vv * ny + ww * nz;
+					const real ub = uu - un * nx, vb = vv - un * ny, wb = ww - un * nz;
 					o[0] = ro;
-					o[1] = 2.0 * ub - uu;
-					o[2] = 2.0 * vb - vv;
-					o[3] = 2.0 * wb - ww;
+					o[1] = K(2.0) * ub - uu;
+					o[2] = K(2.0) * vb - vv;
+					o[3] = K(2.0) * wb - ww;
 					o[4] = pp;
 				} else {
-					const double c = sqrt(p->gamma * pp / ro);
-					const double un = uu * nx + vv * ny + ww * nz;
-					if (fabs(un / c) > 1.0) {
-						if (un < 0.0) {
-							o[0] = 2.0 * fr[0] - ro;
-							o[1] = 2.0 * fr[1] - uu;
-							o[2] = 2.0 * fr[2] - vv;
-							o[3] = 2.0 * fr[3] - ww;
-							o[4] = 2.0 * fr[4] - pp;
+					const real c = r_sqrt(K(p->gamma) * pp / ro);
+					const real un = uu * nx + vv * ny + ww * nz;
+					if (r_fabs(un / c) > K(1.0)) {
+						if (un < K(0.0)) {
+							o[0] = K(2.0) * fr[0] - ro;
+							o[1] = K(2.0) * fr[1] - uu;
+							o[2] = K(2.0) * fr[2] - vv;
+							o[3] = K(2.0) * fr[3] - ww;
+							o[4] = K(2.0) * fr[4] - pp;
 						} else {
 							o[0] = ro;
 							o[1] = uu;
@@ -438,31 +574,31 @@ void e3d_oracle_update_boundary(e3d_oracle_block* b, const e3d_oracle_params* p)
 							o[3] = ww;
 							o[4] = pp;
 						}
-					} else if (un < 0.0) {
-						const double pb = 0.5 * (fr[4] + pp - ro * c * (nx * (fr[1] - uu) + ny * (fr[2] - vv) + nz * (fr[3] - ww)));
-						const double rb = fr[0] + (pb - fr[4]) / (c * c);
-						const double ub = fr[1] - nx * (fr[4] - pb) / (ro * c);
-						const double vb = fr[2] - ny * (fr[4] - pb) / (ro * c);
-						const double wb = fr[3] - nz * (fr[4] - pb) / (ro * c);
-						o[0] = 2.0 * rb - ro;
-						o[1] = 2.0 * ub - uu;
-						o[2] = 2.0 * vb - vv;
-						o[3] = 2.0 * wb - ww;
-						o[4] = 2.0 * pb - pp;
+					} else if (un < K(0.0)) {
+						const real pb = K(0.5) * (fr[4] + pp - ro * c * (nx * (fr[1] - uu) + ny * (fr[2] - vv) + nz * (fr[3] - ww)));
+						const real rb = fr[0] + (pb - fr[4]) / (c * c);
+						const real ub = fr[1] - nx * (fr[4] - pb) / (ro * c);
+						const real vb = fr[2] - ny * (fr[4] - pb) / (ro * c);
+						const real wb = fr[3] - nz * (fr[4] - pb) / (ro * c);
+						o[0] = K(2.0) * rb - ro;
+						o[1] = K(2.0) * ub - uu;
+						o[2] = K(2.0) * vb - vv;
+						o[3] = K(2.0) * wb - ww;
+						o[4] = K(2.0) * pb - pp;
 					} else {
-						const double pb = fr[4];
-						const double rb = ro + (pb - pp) / (c * c);
-						const double ub = uu + nx * (pp - pb) / (ro * c);
-						const double vb = vv + ny * (pp - pb) / (ro * c);
-						const double wb = ww + nz * (pp - pb) / (ro * c);
-						o[0] = 2.0 * rb - ro;
-						o[1] = 2.0 * ub - uu;
-						o[2] = 2.0 * vb - vv;
-						o[3] = 2.0 * wb - ww;
-						o[4] = 2.0 * pb - pp;
+						const real pb = fr[4];
+						const real rb = ro + (pb - pp) / (c * c);
+						const real ub = uu + nx * (pp - pb) / (ro * c);
+						const real vb = vv + ny * (pp - pb) / (ro * c);
+						const real wb = ww + nz * (pp - pb) / (ro * c);
+						o[0] = K(2.0) * rb - ro;
+						o[1] = K(2.0) * ub - uu;
+						o[2] = K(2.0) * vb - vv;
+						o[3] = K(2.0) * wb - ww;
+						o[4] = K(2.0) * pb - pp;
 					}
 				}
-				for (int q = 0; q < 5; q++) V5(b->prim, n, q, ext) = o[q];
+				for (int q = 0; q < 5; q++) V5(b->prim, n, q, ext) = ST(o[q]);
 			}
 		}
 		off += b->marker_size[j];
@@ -548,12 +684,29 @@ int e3d_oracle_iterate(e3d_oracle_block* blocks, int n_blocks, const e3d_oracle_
 	const double* beta = rk_beta(p->stages);
 	if (!alpha) return -1;
 	const double aoa = p->aoa_deg * 4. * atan(1.) / 180;
-	if (first_iter == 0) e3d_oracle_halo(blocks, c, n_connexions);
+	if (first_iter == 0) {
+		e3d_oracle_halo(blocks, c, n_connexions);
+#if FP32_MODEL
+		/* the carried FP64 conservative state starts from the FP64 freestream */
+		double f[5];
+		e3d_oracle_freestream(p, f);
+		for (int bi = 0; bi < n_blocks; bi++) {
+			e3d_oracle_block* b = &blocks[bi];
+			for (int cc = 0; cc < b->n_real; cc++) {
+				V5(b->w0, b->n_all, 0, cc) = f[0];
+				V5(b->w0, b->n_all, 1, cc) = f[0] * f[1];
+				V5(b->w0, b->n_all, 2, cc) = f[0] * f[2];
+				V5(b->w0, b->n_all, 3, cc) = f[0] * f[3];
+				V5(b->w0, b->n_all, 4, cc) = 0.5 * f[0] * (f[1] * f[1] + f[2] * f[2] + f[3] * f[3]) + 1. / (p->gamma - 1.0) * f[4];
+			}
+		}
+#endif
+	}
 	for (int it = 0; it < n_iter; it++) {
 		double rms[5] = {0, 0, 0, 0, 0}, cl = 0, cd = 0, cmx = 0, cmy = 0, cmz = 0;
 		for (int bi = 0; bi < n_blocks; bi++) {
 			e3d_oracle_block* b = &blocks[bi];
-			e3d_oracle_save_w0(b, p);
+			if (!FP32_MODEL) e3d_oracle_save_w0(b, p);
 			e3d_oracle_spectral_radius(b, p);
 			e3d_oracle_timestep(b, p);
 			for (int s = 0; s < p->stages; s++) {
@@ -564,7 +717,7 @@ int e3d_oracle_iterate(e3d_oracle_block* blocks, int n_blocks, const e3d_oracle_
 				e3d_oracle_flux_conv(b, p);
 				e3d_oracle_flux_diss(b, p, beta[s]);
 				if (p->smoothing) e3d_oracle_smooth(b);
-				e3d_oracle_update_internal(b, p, alpha[s]);
+				update_internal(b, p, alpha[s], (FP32_MODEL && s == p->stages - 1) ? b->w0 : 0);
 				e3d_oracle_update_boundary(b, p);
 			}
 			double fd[10];

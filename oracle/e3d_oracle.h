@@ -85,6 +85,11 @@ void e3d_oracle_flow_data(const e3d_oracle_block* b, const e3d_oracle_params* p,
 int e3d_oracle_iterate(e3d_oracle_block* blocks, int n_blocks, const e3d_oracle_connexion* c, int n_connexions,
                        const e3d_oracle_params* p, int n_iter, int first_iter, double* rms0, int* have_rms0,
                        double* hist);
+/* FP32 model library only (libe3d_oracle32.so): with a nonzero seed every
+ * face flux is left as computed (half the cases) or moved one FP32 unit up or
+ * down (a quarter each), by a seeded hash (0: no perturbation; the FP64
+ * library ignores the seed) */
+void e3d_oracle_set_noise(unsigned long long seed);
 
 #ifdef __cplusplus
 }

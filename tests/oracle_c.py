@@ -1,4 +1,5 @@
-"""ctypes driver for the C restatement oracle (oracle/libe3d_oracle.so).
+"""ctypes driver for the C restatement oracle (oracle/libe3d_oracle.so) and for
+the same source built as a model of the FP32 variant (oracle/libe3d_oracle32.so).
 
 Test infrastructure: used by tests/ and by bench.py's CPU-baseline leg only.
 Blocks are assembled from per-block geometry arrays (the reference's own, from
@@ -13,6 +14,7 @@ import numpy as np
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(REPO, "oracle", "libe3d_oracle.so")
+LIB32 = os.path.join(REPO, "oracle", "libe3d_oracle32.so")
 
 DP = C.POINTER(C.c_double)
 IP = C.POINTER(C.c_int)
@@ -40,16 +42,18 @@ class OConn(C.Structure):
                 ("origin_cells", IP)]
 
 
-_lib = None
+_libs: dict = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB):
-            raise ImportError(f"{LIB} missing: run `make -C oracle oracle`")
-        _lib = C.CDLL(LIB)
-    return _lib
+def lib(fp32: bool = False):
+    """The FP64 oracle, or (fp32=True) the model of the FP32 variant."""
+    path = LIB32 if fp32 else LIB
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise ImportError(f"{path} missing: run `make -C oracle oracle`")
+        _libs[path] = C.CDLL(path)
+        _libs[path].e3d_oracle_set_noise.argtypes = [C.c_ulonglong]
+    return _libs[path]
 
 
 def _p(a, t):
@@ -119,7 +123,10 @@ def params_from_deck(d) -> OParams:
 class OracleCase:
     """All blocks of a case plus the connexion lists; runs outer iterations."""
 
-    def __init__(self, blocks: list[OracleBlock], params: OParams, connexions: list[tuple] = ()):
+    def __init__(self, blocks: list[OracleBlock], params: OParams, connexions: list[tuple] = (), fp32: bool = False,
+                 noise_seed: int = 0):
+        self.fp32 = fp32
+        self.noise_seed = noise_seed
         self.blocks = blocks
         self.p = params
         self.arr = (OBlock * len(blocks))(*[b.s for b in blocks])
@@ -136,18 +143,25 @@ class OracleCase:
         self.have_rms0 = C.c_int(0)
         self.iters = 0
         for i in range(len(blocks)):
-            lib().e3d_oracle_init_state(C.byref(self.arr[i]), C.byref(self.p))
+            lib(fp32).e3d_oracle_init_state(C.byref(self.arr[i]), C.byref(self.p))
 
     def iterate(self, n: int) -> np.ndarray:
         hist = np.zeros((n, 15))
-        rc = lib().e3d_oracle_iterate(self.arr, len(self.blocks), self.conns, self.n_conn, C.byref(self.p), n,
-                                      self.iters, self.rms0, C.byref(self.have_rms0), _p(hist, DP))
+        L = lib(self.fp32)
+        if self.fp32:
+            L.e3d_oracle_set_noise(self.noise_seed)  # restarts the seeded sequence
+            if self.iters:
+                raise ValueError("the FP32 model runs its iterations in one call (seeded noise sequence)")
+        rc = L.e3d_oracle_iterate(self.arr, len(self.blocks), self.conns, self.n_conn, C.byref(self.p), n,
+                                  self.iters, self.rms0, C.byref(self.have_rms0), _p(hist, DP))
+        if self.fp32:
+            L.e3d_oracle_set_noise(0)
         assert rc == 0
         self.iters += n
         return hist
 
     def call(self, fn: str, b: int, *args) -> None:
-        getattr(lib(), "e3d_oracle_" + fn)(C.byref(self.arr[b]), *args)
+        getattr(lib(self.fp32), "e3d_oracle_" + fn)(C.byref(self.arr[b]), *args)
 
 
 def connexions_from_topology(path: str, n_real: list[int]) -> list[tuple]:
@@ -181,7 +195,8 @@ def connexions_from_topology(path: str, n_real: list[int]) -> list[tuple]:
     return out
 
 
-def case_oracle(case, top_path: str) -> OracleCase:
+def case_oracle(case, top_path: str, fp32: bool = False, noise_seed: int = 0) -> OracleCase:
     blocks = [OracleBlock.from_case(case, b) for b in range(case.n_blocks)]
     return OracleCase(blocks, params_from_deck(case.deck),
-                      connexions_from_topology(top_path, [b.n_real for b in blocks]))
+                      connexions_from_topology(top_path, [b.n_real for b in blocks]), fp32=fp32,
+                      noise_seed=noise_seed)

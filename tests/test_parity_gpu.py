@@ -5,8 +5,12 @@ Bar: the FP64 path reproduces every reference array exactly (same values; the
 kernels keep the reference's operation order and are built without FMA
 contraction).  Residual norms are sums over cells whose order differs (tree
 reduction on the device, sequential loop in the reference): relative 1e-12.
-The FP32 path is compared with a tolerance stated per quantity.
+The FP32 path is compared with bounds derived from a model of the FP32 build
+(tests/golden/fp32_bounds.json).
 """
+import json
+import os
+
 import numpy as np
 import pytest
 from conftest import Golden, golden_names, max_rel, same
@@ -118,30 +122,37 @@ def test_fused_no_graph_equals_graph(name, tmp_path):
         assert same(s1.get(b, "prim"), s2.get(b, "prim"))
 
 
+FP32_BOUNDS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fp32_bounds.json")
+
+
 @pytest.mark.parametrize("name", golden_names())
 def test_fp32_variant_error(name, tmp_path):
     """FP32 flux/gradient/limiter arithmetic with FP64 conserved state and FP64
     norm/force reductions, against the FP64 reference history.
-    These are 20-30 iteration transients from freestream, during which FP32
-    rounding can flip discrete limiter decisions (min over faces, BJ's fmin)
-    and FP32 storage of near-freestream states makes neighbour differences
-    (gradients) coarse: Cl, Cd within 5e-3 of max(|value|, 1e-2); state within
-    1e-3 relative;
-    density-residual norm within 1e-2 relative (a difference of nearly equal
-    fluxes, the most rounding-sensitive quantity).  The 1e-4 Cl/Cd target for
-    a converged FP32 solution is checked on the full-size workload."""
+    The bounds are derived, per fixture and per iteration, from a model of the
+    FP32 build (tests/golden/make_fp32_bounds.py: the oracle in float working
+    precision, 16 rounding realisations, bound = 2 x their largest deviation,
+    at least 2e-6): density-residual norm relative to the reference's, Cl and
+    Cd relative to max(max |reference|, 1e-2), and the final state relative to
+    max(|reference|, 1).  The 1e-4 Cl/Cd target of a converged FP32 solution
+    is checked on converged runs (tests/test_fullsize_gpu.py)."""
+    bounds = json.load(open(FP32_BOUNDS))["fixtures"][name]
     g, case, s = _open(name, tmp_path, precision="fp32")
     iters = len(g.hist("iter"))
     s.iterate(iters)
     h = s.history()
     for col in ("cl", "cd"):
         scale = max(np.max(np.abs(g.hist(col))), 1e-2)
-        assert np.max(np.abs(h[col] - g.hist(col))) / scale < 5e-3, col
-    assert max_rel(h["rms"][:, 0], g.hist("rms_ro")) < 1e-2
+        dev = np.abs(h[col] - g.hist(col)) / scale
+        assert np.all(dev <= np.array(bounds[col])), (col, int(np.argmax(dev / np.array(bounds[col]))), dev.max())
+    dev = np.abs(h["rms"][:, 0] - g.hist("rms_ro")) / np.abs(g.hist("rms_ro"))
+    assert np.all(dev <= np.array(bounds["rms"])), ("rms", int(np.argmax(dev / np.array(bounds["rms"]))), dev.max())
+    st = 0.0
     for b in range(g.n_blocks):
         p = s.get(b, "prim").reshape(5, -1)
         r = g[f"iter{iters}.b{b}.prim"].reshape(5, -1)
-        assert np.max(np.abs(p - r) / np.maximum(np.abs(r), 1.0)) < 1e-3
+        st = max(st, float(np.max(np.abs(p - r) / np.maximum(np.abs(r), 1.0))))
+    assert st <= bounds["state"], ("state", st, bounds["state"])
 
 
 def test_solve_stops_like_reference(tmp_path):
