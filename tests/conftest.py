@@ -21,12 +21,19 @@ def pytest_configure(config):
 
 
 def golden_names(small_only: bool = True) -> list[str]:
+    """Fixtures on generated meshes with their arrays stored (ref_* excluded)."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    names = [n for n in names if not n.startswith("ref_")]
     if small_only:
         # bump*: full-size histories; irs*: residual smoothing, whose reference run
         # reads an unset array after the first smoothing (dedicated tests)
         names = [n for n in names if not n.startswith(("bump", "irs"))]
     return names
+
+
+def ref_golden_names() -> list[str]:
+    """Fixtures on the reference's own shipped meshes (array hashes, no arrays)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "ref_*.npz")))
 
 
 class Golden:
@@ -44,7 +51,7 @@ class Golden:
 
     @property
     def n_blocks(self):
-        return self.spec.get("blocks", 1)
+        return self.meta.get("blocks", self.spec.get("blocks", 1))
 
     @property
     def stages(self):
@@ -52,13 +59,22 @@ class Golden:
 
     def write_case(self, directory: str) -> str:
         """Regenerate the case files; fails if the generator output drifted."""
-        from euler3d_b200 import meshgen as mg
         sys.path.insert(0, GOLDEN)
+        if "input" in self.spec:  # the reference's own meshes, unpacked from tests/golden/ref_inputs
+            import make_ref_inputs  # noqa: E402
+
+            deck = make_ref_inputs.write_case(self.spec, directory)
+            assert make_ref_inputs.files_sha(directory) == self.meta["sha256"], "reference input files changed"
+            return deck
         import make_golden  # noqa: E402
 
         deck = make_golden.write(self.spec, directory)
         assert make_golden.files_sha(directory) == self.meta["sha256"], "mesh generator output changed"
         return deck
+
+    def hash(self, key: str) -> str:
+        """SHA-256 of a reference array (ref_* fixtures; see make_ref_inputs.array_hash)."""
+        return self.meta["hashes"][key]
 
     def hist(self, col: str) -> np.ndarray:
         return self.z["hist." + col]
@@ -83,6 +99,13 @@ def same(a: np.ndarray, b: np.ndarray) -> bool:
     a = np.asarray(a)
     b = np.asarray(b)
     return a.shape == b.shape and bool(np.all(a == b))
+
+
+def array_hash(a: np.ndarray) -> str:
+    sys.path.insert(0, GOLDEN)
+    import make_ref_inputs  # noqa: E402
+
+    return make_ref_inputs.array_hash(a)
 
 
 def max_rel(a: np.ndarray, b: np.ndarray, floor: float = 1e-300) -> float:
