@@ -38,6 +38,7 @@ UNIT = "cell-iterations/s"
 WORKLOAD = dict(n=80, blocks=16, order=2, flux="roe", gradient="leastsquares", limiter="venkatakrishnan", k=5.0,
                 omega=2.16e-16, mach=0.7, aoa_deg=1.25, cfl=1.5, stages=5)
 REFDRIVER = os.path.join(HERE, "oracle", "_ref", "e3d_refdriver")
+RENUMBER = "none"  # device cell order of the channel workload (e3d_options.renumber)
 
 
 def log(*a):
@@ -456,6 +457,12 @@ def main():
                          "into a temporary directory when absent")
     ap.add_argument("--scale", choices=["full", "small"], default="full",
                     help="small: the same sweep workloads on 10^3..16^3 meshes (quick checks)")
+    ap.add_argument("--renumber", choices=["none", "rcm", "morton", "shuffle"], default=RENUMBER,
+                    help="device order of each block's real cells (e3d_options.renumber)")
+    ap.add_argument("--no-error-report", action="store_true",
+                    help="channel, fp32: skip the FP32-vs-FP64 error report (profiling runs)")
+    ap.add_argument("--fp64-steps", type=int, default=50,
+                    help="channel, fp32: also time this many steps of the FP64 bitwise drop-in path (0: skip)")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -485,10 +492,12 @@ def main():
         else:
             deck, case_dir = make_case(td, a.n, a.blocks), td
             cfg = workload_config(a.n, a.blocks, a.precision)
+        cfg["cell_order"] = a.renumber
         t1 = time.time()
         case = Case(deck)
         t2 = time.time()
-        s = Solver(case, precision=a.precision, device=local, hist_capacity=max(4096, a.steps + 64))
+        s = Solver(case, precision=a.precision, device=local, hist_capacity=max(4096, a.steps + 64),
+                   renumber=a.renumber)
         t3 = time.time()
         log(f"[bench] rank {rank}: mesh gen {t1 - t0:.1f}s, case load {t2 - t1:.1f}s, solver setup {t3 - t2:.1f}s, "
             f"device bytes {s.device_bytes() / 1e9:.2f} GB")
@@ -568,8 +577,29 @@ def main():
         # timestamp in this query: keep all samples of the measured run)
         cl = ClockSampler.summarize(rows)
 
+        # the FP64 bitwise drop-in path (the reference's arithmetic) on the same
+        # workload, timed the same way: its own solver, warm-up, CUDA events
+        fp64_path = None
+        if a.precision == "fp32" and a.workload == "channel" and a.fp64_steps > 0:
+            s64 = Solver(case, precision="fp64", device=local, hist_capacity=max(4096, a.fp64_steps + 64),
+                         renumber=a.renumber)
+            s64.iterate(warm)
+            s64.sync()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            ms64 = s64.iterate_timed(a.fp64_steps)
+            torch.cuda.synchronize()
+            c64 = combine_ranks(ms64, cells, a.fp64_steps, world, dist if world > 1 else None, device="cuda")
+            kt64 = s64.time_kernels(5)
+            fp64_path = {"value": c64["value"], "unit": UNIT, "ms_per_step": c64["ms"] / a.fp64_steps,
+                         "steps": a.fp64_steps, "warmup": warm, "dtype": "f64",
+                         "note": "the drop-in path: every array bit for bit the reference's",
+                         "kernels_gbs": {k["name"]: (k["bytes_per_launch"] / (k["total_ms"] / k["launches"] / 1000.0)
+                                                     / 1e9) if k["bytes_per_launch"] else None for k in kt64}}
+            s64.close()
         fp32_err = None
-        if rank == 0 and a.precision == "fp32" and a.workload == "channel":
+        if rank == 0 and a.precision == "fp32" and a.workload == "channel" and not a.no_error_report:
             fp32_err = fp32_error_report(td)
         cpu = None
         if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -586,7 +616,7 @@ def main():
             "clocks": cl,
             "final": {"iterations": int(len(hist["iter"])), "ro_conv": float(hist["conv"][-1, 0]),
                       "cl": float(hist["cl"][-1]), "cd": float(hist["cd"][-1])},
-            "fp32_vs_fp64": fp32_err}
+            "fp32_vs_fp64": fp32_err, "fp64_path": fp64_path}
     if rank == 0:
         print(json.dumps(line))
     s.close()

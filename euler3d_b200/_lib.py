@@ -22,6 +22,7 @@ GRAD = {"greengauss": 0, "leastsquares": 1}
 LIM = {"barthjespersen": 0, "venkatakrishnan": 1}
 FLUX = {"roe": 0, "ausm": 1}
 FP64, FP32, FP64_FMA = 0, 1, 2
+RENUMBER = {"none": 0, "rcm": 1, "morton": 2, "shuffle": 3}  # e3d_options.renumber
 SURROGATE_PARAMS, SURROGATE_NORM = 36232, 24
 
 
@@ -45,7 +46,7 @@ class BlockInfo(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("carry_w0", C.c_int), ("use_graph", C.c_int), ("device", C.c_int),
-                ("stream", C.c_void_p), ("hist_capacity", C.c_int)]
+                ("stream", C.c_void_p), ("hist_capacity", C.c_int), ("renumber", C.c_int)]
 
 
 class IterRecord(C.Structure):
@@ -68,6 +69,7 @@ SIGNATURES = {
     "e3d_case_block_info": ([C.c_void_p, C.c_int, C.POINTER(BlockInfo)], C.c_int),
     "e3d_case_get_f64": ([C.c_void_p, C.c_int, C.c_char_p, C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
     "e3d_case_get_i32": ([C.c_void_p, C.c_int, C.c_char_p, C.c_void_p, C.POINTER(C.c_int64)], C.c_int),
+    "e3d_case_cell_order": ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64], C.c_int),
     "e3d_solver_create": ([C.c_void_p, C.POINTER(Options), C.POINTER(C.c_void_p)], C.c_int),
     "e3d_solver_free": ([C.c_void_p], C.c_int),
     "e3d_solver_sync": ([C.c_void_p], C.c_int),

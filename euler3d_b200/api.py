@@ -58,6 +58,13 @@ class Case:
         L.check(fn(self._h, b, name.encode(), L.ptr(out), C.byref(n)))
         return out
 
+    def cell_order(self, b: int, mode: str) -> np.ndarray:
+        """order[i] = file index of the real cell a solver with renumber=mode places i-th."""
+        n = self.block_info(b).n_real
+        out = np.empty(n, dtype=np.int32)
+        L.check(L.lib().e3d_case_cell_order(self._h, b, L.RENUMBER[mode], L.ptr(out), n))
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
             L.lib().e3d_case_free(self._h)
@@ -74,7 +81,7 @@ class Solver:
     """Device-resident solver over every block of a case."""
 
     def __init__(self, case: Case, precision: str = "fp64", carry_w0: int = -1, use_graph: bool = True,
-                 device: int = -1, stream: int | None = None, hist_capacity: int = 4096):
+                 device: int = -1, stream: int | None = None, hist_capacity: int = 4096, renumber: str = "none"):
         lib = L.lib()
         o = L.Options()
         lib.e3d_default_options(C.byref(o))
@@ -84,6 +91,7 @@ class Solver:
         o.device = device
         o.stream = stream
         o.hist_capacity = hist_capacity
+        o.renumber = L.RENUMBER[renumber]
         h = C.c_void_p()
         L.check(lib.e3d_solver_create(case._h, C.byref(o), C.byref(h)))
         self._h = h
@@ -207,7 +215,7 @@ class Batch(Solver):
     """Several cases advanced together (one device arena, persistent kernel)."""
 
     def __init__(self, cases: list, precision: str = "fp32", use_graph: bool = True, device: int = -1,
-                 hist_capacity: int = 4096):
+                 hist_capacity: int = 4096, renumber: str = "none"):
         lib = L.lib()
         o = L.Options()
         lib.e3d_default_options(C.byref(o))
@@ -215,6 +223,7 @@ class Batch(Solver):
         o.use_graph = 1 if use_graph else 0
         o.device = device
         o.hist_capacity = hist_capacity
+        o.renumber = L.RENUMBER[renumber]
         arr = (C.c_void_p * len(cases))(*[c._h.value for c in cases])
         h = C.c_void_p()
         L.check(lib.e3d_batch_create(arr, len(cases), C.byref(o), C.byref(h)))

@@ -71,6 +71,7 @@ void e3d_default_options(e3d_options* o) {
 	o->device = -1;
 	o->stream = nullptr;
 	o->hist_capacity = 4096;
+	o->renumber = E3D_RENUMBER_NONE;
 }
 
 int e3d_case_load(const char* deck_path, const char* workdir, e3d_case** out) {
@@ -159,6 +160,16 @@ int e3d_case_get_f64(const e3d_case* c, int block, const char* name, double* dst
 	});
 }
 
+int e3d_case_cell_order(const e3d_case* c, int block, int mode, int32_t* order, int64_t n_real) {
+	if (!order) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		const e3d::HostBlock& B = block_of(c, block);
+		if (n_real != B.n_real) throw e3d::Error(E3D_ERR_ARG, "order: wrong count");
+		const std::vector<int> o = e3d::cell_order(B, mode);
+		std::copy(o.begin(), o.end(), order);
+	});
+}
+
 int e3d_case_get_i32(const e3d_case* c, int block, const char* name, int32_t* dst, int64_t* count) {
 	if (!name || !count) return fail(E3D_ERR_ARG, "null argument");
 	return guard([&] {
@@ -203,6 +214,7 @@ int e3d_solver_create(const e3d_case* c, const e3d_options* opt, e3d_solver** ou
 		eo.device = o.device;
 		eo.stream = static_cast<cudaStream_t>(o.stream);
 		eo.hist_capacity = o.hist_capacity > 0 ? (size_t)o.hist_capacity : 4096;
+		eo.renumber = o.renumber;
 		auto* s = new e3d_solver;
 		try {
 			s->eng.reset(new e3d::Engine(c->hc, eo));
@@ -233,6 +245,7 @@ int e3d_batch_create(const e3d_case* const* cases, int n_cases, const e3d_option
 		eo.device = o.device;
 		eo.stream = static_cast<cudaStream_t>(o.stream);
 		eo.hist_capacity = o.hist_capacity > 0 ? (size_t)o.hist_capacity : 4096;
+		eo.renumber = o.renumber;
 		auto* s = new e3d_solver;
 		try {
 			s->eng.reset(new e3d::Engine(list, eo));

@@ -202,9 +202,17 @@ void Engine::build_blocks(const std::vector<const HostBlock*>& blocks, const std
 	NG_ = goff_[nb_];
 	NA_ = NR_ + NG_;
 	NF_ = foff_[nb_];
+	// device order of each block's real cells (identity unless renumbered)
+	pos_.assign(nb_, {});
+	for (int b = 0; b < nb_; b++) {
+		const HostBlock& B = hc.blocks[b];
+		pos_[b].resize(B.n_real);
+		const std::vector<int> order = cell_order(B, opt_.renumber);
+		for (int i = 0; i < B.n_real; i++) pos_[b][order[i]] = i;
+	}
 	auto gid = [&](int b, int local) {
 		const HostBlock& B = hc.blocks[b];
-		return local < B.n_real ? roff_[b] + local : NR_ + goff_[b] + (local - B.n_real);
+		return local < B.n_real ? roff_[b] + pos_[b][local] : NR_ + goff_[b] + (local - B.n_real);
 	};
 	// slots, in global cell order
 	std::vector<int> slot_ptr(NA_ + 1, 0);
@@ -313,7 +321,7 @@ void Engine::build_blocks(const std::vector<const HostBlock*>& blocks, const std
 		for (int b = 0; b < nb_; b++) {
 			const HostBlock& B = hc.blocks[b];
 			for (int c = 0; c < B.n_real; c++)
-				for (int d = 0; d < 3; d++) cen[3 * (size_t)(roff_[b] + c) + d] = (float)B.cell_center[3 * (size_t)c + d];
+				for (int d = 0; d < 3; d++) cen[3 * (size_t)gid(b, c) + d] = (float)B.cell_center[3 * (size_t)c + d];
 		}
 		cen_d_.upload(cen);
 		block_case_d_.upload(block_case_);
@@ -1029,6 +1037,28 @@ void h2d_rows(T* dev, int ld, int rows, int begin, int count, const std::vector<
 // Names and layouts match the reference's arrays for block `block`:
 //   prim [5][n_all], limiter [5][n_all], grad [5][n_all][3],
 //   conv_res/diss_res/w0 [5][n_real], dt/spectral_radius [n_real]
+// Real cells of block b sit on the device in the order pos_[b]; these move
+// the first nr entries of each of `rows` rows of length ld between device
+// order and the block's local (file) order.
+void Engine::to_local(int b, std::vector<double>& a, int rows, int ld) const {
+	const std::vector<int>& pos = pos_[b];
+	std::vector<double> t(pos.size());
+	for (int q = 0; q < rows; q++) {
+		double* r = a.data() + (size_t)q * ld;
+		for (size_t c = 0; c < pos.size(); c++) t[c] = r[pos[c]];
+		std::copy(t.begin(), t.end(), r);
+	}
+}
+void Engine::to_device(int b, std::vector<double>& a, int rows, int ld) const {
+	const std::vector<int>& pos = pos_[b];
+	std::vector<double> t(pos.size());
+	for (int q = 0; q < rows; q++) {
+		double* r = a.data() + (size_t)q * ld;
+		for (size_t c = 0; c < pos.size(); c++) t[pos[c]] = r[c];
+		std::copy(t.begin(), t.end(), r);
+	}
+}
+
 void Engine::get(const std::string& name, int b, std::vector<double>& out) {
 	if (b < 0 || b >= nb_) throw Error(E3D_ERR_ARG, "block index out of range");
 	cuda_ok(cudaStreamSynchronize(st_), "sync");
@@ -1038,15 +1068,18 @@ void Engine::get(const std::string& name, int b, std::vector<double>& out) {
 		out.assign((size_t)rows * na, 0.0);
 		d2h_rows(dev, NA_, rows, r0, nr, out, 0, na, st_);
 		d2h_rows(dev, NA_, rows, g0, ng, out, nr, na, st_);
+		to_local(b, out, rows, na);
 	};
 	auto rows_real = [&](int rows, auto* dev) {
 		out.assign((size_t)rows * nr, 0.0);
 		d2h_rows(dev, NR_, rows, r0, nr, out, 0, nr, st_);
+		to_local(b, out, rows, nr);
 	};
 	auto packed_all = [&](auto* dev) {
 		out.assign((size_t)5 * na, 0.0);
 		d2h_packed(dev, NA_, r0, nr, out, 0, na, st_);
 		d2h_packed(dev, NA_, g0, ng, out, nr, na, st_);
+		to_local(b, out, 5, na);
 	};
 	if (name == "prim") {
 		if (f64) packed_all(cur_ ? f64_.P1.p : f64_.P0.p);
@@ -1083,24 +1116,31 @@ void Engine::get(const std::string& name, int b, std::vector<double>& out) {
 	}
 }
 
-void Engine::set(const std::string& name, int b, const std::vector<double>& in) {
+void Engine::set(const std::string& name, int b, const std::vector<double>& in_local) {
 	if (b < 0 || b >= nb_) throw Error(E3D_ERR_ARG, "block index out of range");
 	cuda_ok(cudaStreamSynchronize(st_), "sync");
 	const int nr = n_real_b_[b], na = n_all_b_[b], ng = na - nr, r0 = roff_[b], g0 = NR_ + goff_[b];
 	const bool f64 = opt_.precision == PREC_FP64;
+	std::vector<double> in(in_local);  // real cells moved to device order below
 	auto put_all = [&](int rows, auto* dev) {
 		if (in.size() != (size_t)rows * na) throw Error(E3D_ERR_ARG, name + ": wrong length");
+		to_device(b, in, rows, na);
 		h2d_rows(dev, NA_, rows, r0, nr, in, 0, na, st_);
 		h2d_rows(dev, NA_, rows, g0, ng, in, nr, na, st_);
+		in = in_local;
 	};
 	auto put_real = [&](int rows, auto* dev) {
 		if (in.size() != (size_t)rows * nr) throw Error(E3D_ERR_ARG, name + ": wrong length");
+		to_device(b, in, rows, nr);
 		h2d_rows(dev, NR_, rows, r0, nr, in, 0, nr, st_);
+		in = in_local;
 	};
 	auto put_packed = [&](auto* dev) {
 		if (in.size() != (size_t)5 * na) throw Error(E3D_ERR_ARG, name + ": wrong length");
+		to_device(b, in, 5, na);
 		h2d_packed(dev, NA_, r0, nr, in, 0, na, st_);
 		h2d_packed(dev, NA_, g0, ng, in, nr, na, st_);
+		in = in_local;
 	};
 	if (name == "prim") {
 		// both ping-pong buffers, so ghost cells that no stage rewrites stay consistent
@@ -1132,6 +1172,7 @@ void Engine::set(const std::string& name, int b, const std::vector<double>& in) 
 		for (int q = 0; q < 5; q++)
 			for (int c = 0; c < na; c++)
 				for (int d = 0; d < 3; d++) t[(size_t)(q * 3 + d) * na + c] = in[((size_t)q * na + c) * 3 + d];
+		to_device(b, t, 15, na);
 		h2d_rows(grad_.p, NA_, 15, r0, nr, t, 0, na, st_);
 		h2d_rows(grad_.p, NA_, 15, g0, ng, t, nr, na, st_);
 	} else {

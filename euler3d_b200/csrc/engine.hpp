@@ -21,7 +21,15 @@ struct EngineOptions {
 	int device = -1;     // -1: current device
 	cudaStream_t stream = nullptr;  // nullptr: the engine creates its own stream
 	size_t hist_capacity = 4096;    // iterations of per-block norm/force history kept on device
+	int renumber = 0;    // RENUMBER_*: device order of each block's real cells
 };
+
+// Device order of the real cells inside each block (renumber.cpp).  Slots keep
+// each cell's ascending face order, so every per-cell sum runs in the
+// reference's order whatever the cell order.
+enum Renumber : int { RENUMBER_NONE = 0, RENUMBER_RCM = 1, RENUMBER_MORTON = 2, RENUMBER_SHUFFLE = 3 };
+// order[i] = block-local real cell placed i-th on the device
+std::vector<int> cell_order(const HostBlock& b, int mode);
 
 // Host copy of one outer iteration's results (reference PostProcessing fields).
 struct IterRecord {
@@ -155,6 +163,8 @@ private:
 	};
 	void setup(const std::vector<const HostCase*>& cases);
 	void build_blocks(const std::vector<const HostBlock*>& blocks, const std::vector<Connexion>& conns);
+	void to_local(int b, std::vector<double>& a, int rows, int ld) const;
+	void to_device(int b, std::vector<double>& a, int rows, int ld) const;
 	void init_state();
 	void count_device_bytes();
 	void check(const char* what);
@@ -176,6 +186,7 @@ private:
 	int nb_ = 0, NR_ = 0, NG_ = 0, NA_ = 0, NF_ = 0, NS_ = 0, tet4_ = 0;
 	std::vector<int> roff_, goff_, foff_, soff_;  // per block offsets (nb_+1)
 	std::vector<int> n_real_b_, n_all_b_;
+	std::vector<std::vector<int>> pos_;  // per block: device position (0..n_real-1) of each local real cell
 	Physics ph_{};
 	double denom_ = 1.0, aoa_rad_ = 0.0;
 	int ncases_ = 1;

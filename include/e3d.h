@@ -57,6 +57,17 @@ typedef struct e3d_block_info {
 	int n_real, n_all, n_faces, n_nodes, n_markers, n_real_boundaries, n_wall_faces;
 } e3d_block_info;
 
+/* device order of each block's real cells (e3d_options.renumber).  No
+ * counterpart in the reference, which keeps file order.  A cell's slots keep
+ * its ascending face order, so FP64 results are bit for bit the same in every
+ * order; state transfers (e3d_state_get/set) stay in file order.  The state
+ * blob of e3d_state_export and the rows of e3d_cell_features are in device
+ * order. */
+#define E3D_RENUMBER_NONE 0    /* file order */
+#define E3D_RENUMBER_RCM 1     /* reverse Cuthill-McKee on the cell adjacency graph */
+#define E3D_RENUMBER_MORTON 2  /* Z-order curve of the cell centres */
+#define E3D_RENUMBER_SHUFFLE 3 /* seeded random order (worst case, for tests and measurement) */
+
 typedef struct e3d_options {
 	int precision;    /* E3D_FP64 or E3D_FP32 */
 	int carry_w0;     /* -1 default (FP32: on), 0 recompute W0 from primitives, 1 carry FP64 W */
@@ -64,6 +75,7 @@ typedef struct e3d_options {
 	int device;       /* -1: current device */
 	void* stream;     /* cudaStream_t or NULL (solver creates its own) */
 	int hist_capacity;/* iterations of history buffered on the device (0: 4096) */
+	int renumber;     /* E3D_RENUMBER_* (default E3D_RENUMBER_NONE) */
 } e3d_options;
 
 /* One outer iteration's post-processing (PostProcessing::process,
@@ -102,6 +114,10 @@ int e3d_case_block_info(const e3d_case* c, int block, e3d_block_info* out);
  * cell_faces, cell_cells, wall_faces, marker_kind, marker_size, marker_cells. */
 int e3d_case_get_f64(const e3d_case* c, int block, const char* name, double* dst, int64_t* count);
 int e3d_case_get_i32(const e3d_case* c, int block, const char* name, int32_t* dst, int64_t* count);
+/* The device order a solver created with e3d_options.renumber = mode gives the
+ * real cells of one block: order[i] = block-local (file) index of the cell
+ * placed i-th (n_real entries).  Host only.  No counterpart in the reference. */
+int e3d_case_cell_order(const e3d_case* c, int block, int mode, int32_t* order, int64_t n_real);
 
 /* ---- solver ------------------------------------------------------------------
  * e3d_solver_create replaces Initializer::initializeSolver
@@ -198,7 +214,8 @@ int e3d_batch_tuning(const e3d_solver* s, int* tile_cells, int* grid, double* ms
  * residual stops dropping near 5 orders (FP32 rounding of the fluxes); a run
  * to a deeper drop continues in FP64 from there.
  * e3d_cell_features: surrogate inputs of every real cell of every case, in
- * device cell order (blocks in order, real cells in file order), 8 floats per
+ * device cell order (blocks in order, real cells in the order that
+ * e3d_options.renumber chose; file order by default), 8 floats per
  * cell: centroid x y z, distance to the nearest wall-face centre of the
  * cell's case, Mach, alpha (deg), 0, 0.
  * The surrogate is a 4-layer MLP 6 -> 128 -> 128 -> 128 -> 5 with exact-erf

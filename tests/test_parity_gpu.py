@@ -112,6 +112,78 @@ def test_fused_fp64_matches_reference(name, tmp_path):
     assert np.max(np.abs(h["conv"][:, 0] - g.hist("ro_conv"))) < 1e-11
 
 
+@pytest.mark.parametrize("renumber", ["rcm", "morton", "shuffle"])
+@pytest.mark.parametrize("name", golden_names())
+def test_fused_fp64_any_cell_order(name, renumber, tmp_path):
+    """Renumbering moves where a cell's data sits on the device, not the order
+    of any per-cell sum: the reference's arrays after every golden iteration's
+    end, bit for bit, whatever the device order of the cells."""
+    g, case, s = _open(name, tmp_path, renumber=renumber)
+    iters = len(g.hist("iter"))
+    s.iterate(iters)
+    h = s.history()
+    for b in range(g.n_blocks):
+        assert same(s.get(b, "prim"), g[f"iter{iters}.b{b}.prim"]), b
+        n_real, n_all = case.block_info(b).n_real, case.block_info(b).n_all
+        assert same(s.get(b, "conv_res").reshape(5, n_real), _ref5(g, f"iter{iters}.b{b}.conv_res", n_all, n_real))
+    for col in ("cl", "cd", "cmx", "cmy", "cmz"):
+        assert same(h[col], g.hist(col)), col
+    assert max_rel(h["rms"][:, 0], g.hist("rms_ro")) < RMS_RTOL
+
+
+@pytest.mark.parametrize("name", ["t4_o2_ls_venk_roe_b2", "h5_o2_ls_venk_roe", "t3_o2_gg_bj_ausm"])
+def test_strategy_calls_in_shuffled_cell_order(name, tmp_path):
+    """The granular kernels and the state transfers under a shuffled device
+    order: the reference's arrays after every stage (file order on the host)."""
+    g, case, s = _open(name, tmp_path, renumber="shuffle")
+    rsol = api.ReferenceSolver(s)
+    rk = rsol.runge_kutta_
+    api.halo(s)
+    for b in range(g.n_blocks):
+        blk = api.Block(s, b)
+        api.save_w0(blk)
+        rsol.timestep_.computeSpectralRadius(blk)
+        rsol.timestep_.computeTimestep(blk)
+        for st in range(g.stages):
+            rk.residual_calculator_.current_stage_ = st
+            rk.residual_calculator_.computeResidual(blk)
+            pre = f"it0.s{st}.res.b{b}."
+            assert same(s.get(b, "dt"), g[pre + "dt"]), (b, st, "dt")
+            if g.spec["deck"]["order"] == 2:
+                assert same(s.get(b, "grad"), g[pre + "grad"]), (b, st, "grad")
+                assert same(s.get(b, "limiter"), g[pre + "limiter"]), (b, st, "limiter")
+            rk.updater_.current_stage_ = st
+            rk.updater_.updateInternalBlock(blk)
+            rk.updater_.updateBoundary(blk)
+            assert same(s.get(b, "prim"), g[f"it0.s{st}.upd.b{b}.prim"]), (b, st, "prim")
+    # a state written in file order reads back in file order
+    p = s.get(0, "prim") * 1.0001
+    s.set(0, "prim", p)
+    assert same(s.get(0, "prim"), p)
+
+
+@pytest.mark.parametrize("name", ["t4_o2_ls_venk_roe_b2", "t3_o2_ls_bj_ausm"])
+def test_fp32_same_in_any_cell_order(name, tmp_path):
+    """Per-cell FP32 arithmetic does not depend on where the cell sits: the
+    FP32 states are identical in file order and in a shuffled order."""
+    g, _, a = _open(name, tmp_path / "a", precision="fp32")
+    _, _, b = _open(name, tmp_path / "b", precision="fp32", renumber="shuffle")
+    a.iterate(10)
+    b.iterate(10)
+    for blk in range(g.n_blocks):
+        assert same(a.get(blk, "prim"), b.get(blk, "prim")), blk
+
+
+def test_batch_in_shuffled_cell_order(tmp_path):
+    g = Golden("t4_o2_ls_venk_roe_b2")
+    case = api.Case(g.write_case(str(tmp_path)))
+    b = api.Batch([case, case], precision="fp64", renumber="shuffle")
+    b.solve_batch(1, -1e300, iters_per_launch=1)
+    for c in range(2):
+        for blk in range(g.n_blocks):
+            assert same(b.get(c * g.n_blocks + blk, "prim"), g[f"iter1.b{blk}.prim"]), (c, blk)
+
+
 @pytest.mark.parametrize("name", ["t4_o2_ls_venk_roe_b2", "t3_o2_gg_bj_ausm", "t3_o1_roe", "h5_o2_ls_venk_roe"])
 def test_fused_no_graph_equals_graph(name, tmp_path):
     g, case, s1 = _open(name, tmp_path / "a")

@@ -86,6 +86,20 @@ def test_fused_fp64_on_reference_meshes(name, tmp_path):
         assert np.array_equal(h[col], g.hist(col)), col
 
 
+@pytest.mark.parametrize("renumber", ["rcm", "morton"])
+@pytest.mark.parametrize("name", ["ref_naca_o2_gg_bj_ausm", "ref_onera_o2_ls_venk_roe"])
+def test_fused_fp64_renumbered_on_reference_meshes(name, renumber, tmp_path):
+    """Renumbered device order on the reference's meshes: the same arrays."""
+    g, case, s = _open(name, tmp_path, renumber=renumber)
+    n = len(g.hist("iter"))
+    s.iterate(n)
+    h = s.history()
+    for b in range(g.n_blocks):
+        assert array_hash(s.get(b, "prim")) == g.hash(f"iter{n}.b{b}.prim"), b
+    for col in ("cl", "cd"):
+        assert np.array_equal(h[col], g.hist(col)), col
+
+
 @pytest.mark.parametrize("name", ref_golden_names())
 def test_fp32_variant_on_reference_meshes(name, tmp_path):
     """The FP32 variant against the reference history (bounds derived per
