@@ -21,9 +21,10 @@ def pytest_configure(config):
 
 
 def golden_names(small_only: bool = True) -> list[str]:
-    """Fixtures on generated meshes with their arrays stored (ref_* excluded)."""
+    """Fixtures on generated meshes with their arrays stored (ref_* and the
+    batch fixture batch_* excluded)."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
-    names = [n for n in names if not n.startswith("ref_")]
+    names = [n for n in names if not n.startswith(("ref_", "batch_"))]
     if small_only:
         # bump*: full-size histories; irs*: residual smoothing, whose reference run
         # reads an unset array after the first smoothing (dedicated tests)

@@ -1,10 +1,12 @@
 """Batches of cases (Mach / alpha sweeps on meshes of uneven size).
 
 A batch holds every block of every case in one device arena, each case with its
-own freestream.  The bar is the single-case solver: in FP64 every case of a
-batch must follow, bit for bit, the primitives and Cl/Cd of the same case
-solved alone, through both batch paths (the per-pass graph of e3d_iterate and
-the persistent cooperative kernel of e3d_batch_solve).  Residual norms are
+own freestream.  The bar is the reference run on each case alone (the
+batch_polar3 fixture, uneven meshes and freestreams) and, for more schemes,
+the single-case solver: in FP64 every case of a batch must follow, bit for
+bit, the primitives and Cl/Cd of the same case solved alone, through both
+batch paths (the per-pass graph of e3d_iterate and the persistent cooperative
+kernel of e3d_batch_solve).  Residual norms are
 summed per tile in the persistent kernel, so they match within 1e-12.
 """
 import numpy as np
@@ -78,6 +80,51 @@ def test_batch_persistent_matches_single_cases_fp64(tmp_path, monkeypatch, opts,
     fb = 0
     for c, case in enumerate(cases):
         _check_case(batch, c, fb, _single(case, "fp64", 12))
+        fb += case.n_blocks
+
+
+@pytest.mark.parametrize("form", ["persistent", "per-pass", "graph"])
+def test_batch_matches_the_reference_run_case_by_case(tmp_path, monkeypatch, form):
+    """Uneven meshes and freestreams in one batch, against the reference run
+    on each case alone (tests/golden/batch_polar3.npz): every block's
+    primitives after the first and the last iteration bit for bit, Cl/Cd
+    identical, residual norms within 1e-12 (summation order)."""
+    import json
+    import os
+    import sys
+
+    from conftest import GOLDEN
+
+    sys.path.insert(0, GOLDEN)
+    import make_batch_golden as mbg
+
+    z = np.load(os.path.join(GOLDEN, mbg.NAME + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    cases = [api.Case(mbg.write_case(str(tmp_path / f"c{i}"), i)) for i in range(len(meta["cases"]))]
+    batch = api.Batch(cases, precision="fp64")
+    n = meta["iters"]
+    if form == "graph":  # e3d_iterate on a batch: every case advances together
+        batch.iterate(1)
+    else:
+        monkeypatch.setenv("E3D_BATCH_FORM", form)
+        batch.solve_batch(1, NEVER, iters_per_launch=1)
+    fb = 0
+    for c, case in enumerate(cases):
+        for b in range(case.n_blocks):
+            assert same(batch.get(fb + b, "prim"), z[f"c{c}.iter1.b{b}.prim"]), (c, b)
+        fb += case.n_blocks
+    if form == "graph":
+        batch.iterate(n - 1)
+    else:
+        batch.solve_batch(n, NEVER, iters_per_launch=3)
+    fb = 0
+    for c, case in enumerate(cases):
+        for b in range(case.n_blocks):
+            assert same(batch.get(fb + b, "prim"), z[f"c{c}.iter{n}.b{b}.prim"]), (c, b)
+        h = batch.case_history(c)
+        for col in ("cl", "cd"):
+            assert same(h[col], z[f"c{c}.hist.{col}"]), (c, col)
+        assert max_rel(h["rms"][:, 0], z[f"c{c}.hist.rms_ro"]) < 1e-12
         fb += case.n_blocks
 
 
