@@ -39,6 +39,8 @@ WORKLOAD = dict(n=80, blocks=16, order=2, flux="roe", gradient="leastsquares", l
                 omega=2.16e-16, mach=0.7, aoa_deg=1.25, cfl=1.5, stages=5)
 REFDRIVER = os.path.join(HERE, "oracle", "_ref", "e3d_refdriver")
 RENUMBER = "none"  # device cell order of the channel workload (e3d_options.renumber)
+# the warm-start surrogate trained on the seeded channel sweep (python -m euler3d_b200.sweep train --out ...)
+WARM_DATA = os.path.join(HERE, "euler3d_b200", "data", "warmstart_channel_ausm1.npz")
 
 
 def log(*a):
@@ -299,7 +301,6 @@ def combine_ranks(local_ms: float, cells: int, steps: int, world: int, dist=None
 # ------------------------------------------------------------------ sweep workloads
 POLAR_SCHEME = dict(order=2, flux="ausm", gradient="greengauss", limiter="barthjespersen", omega=2.16e-16, stages=5,
                     cfl=1.5)
-WARM_SCHEME = dict(order=1, flux="ausm", stages=5, cfl=1.5)
 
 
 def _ref_sample(decks, iters, procs):
@@ -326,6 +327,44 @@ def _ref_sample(decks, iters, procs):
                       f"iterations each, reference solver compiled from its sources (-O2, fast face builder); "
                       f"aggregate = sum(cells x iterations) / slowest solve time",
             "wall_s": time.perf_counter() - t0}
+
+
+def warmstart_bounded(n_cases: int = 4, n_max: int = 32) -> dict:
+    """Time to an 8-order density drop, bounded to fit the default run: the
+    first `n_cases` held-out cases of the warm-start sweep with at most n_max^3
+    x 6 tetrahedra, solved by the plain FP64 drop-in path case after case and
+    by one batch with the committed surrogate's warm start (FP32 to -5, then
+    contracted FP64).  The same per-case stop rule and reference residual as
+    `--workload warmstart`, on fewer and smaller cases."""
+    from euler3d_b200 import api
+    from euler3d_b200 import sweep as sw
+
+    if not os.path.exists(WARM_DATA):
+        return {"unavailable": f"{os.path.relpath(WARM_DATA, HERE)} missing"}
+    specs = [p for p in sw.polar_specs(sw.HELD_OUT_SEED, 32, n_range=(25, 60), prefix="test") if p.n <= n_max]
+    specs = specs[:n_cases]
+    crit, max_iter = -8.0, 200000
+    with tempfile.TemporaryDirectory() as td:
+        decks = sw.write_cases(td, specs, sw.WARM_SCHEME, sides="channel", processes=1)
+        cases = [api.Case(d) for d in decks]
+        m, info = sw.load_surrogate(WARM_DATA)
+        learned = sw.solve_batched(cases, crit, max_iter, surrogate=m)
+        plain = [sw.solve_plain(c, crit, max_iter) for c in cases]
+        m.close()
+        for c in cases:
+            c.close()
+    t_plain = sum(p["wall_s"] for p in plain)
+    dcl = max(abs(l["cl"] - p["cl"]) / max(abs(p["cl"]), 1e-2) for l, p in zip(learned["cases"], plain))
+    dcd = max(abs(l["cd"] - p["cd"]) / max(abs(p["cd"]), 1e-2) for l, p in zip(learned["cases"], plain))
+    return {"metric": "time to 1e-8 density-residual drop (s)", "unit": "s", "higher_is_better": False,
+            "cases": [dict(n=p.n, mach=round(p.mach, 4), aoa_deg=round(p.aoa_deg, 4)) for p in specs],
+            "cells": sum(p["cells"] for p in plain), "plain_s": t_plain, "batched_learned_s": learned["wall_s"],
+            "speedup": t_plain / learned["wall_s"], "iters_plain": [p["reached"] for p in plain],
+            "iters_learned": [c["reached"] for c in learned["cases"]], "max_rel_dcl": dcl, "max_rel_dcd": dcd,
+            "phases": learned["phases"], "surrogate": {k: info.get(k) for k in ("cases", "train_seed", "loss")},
+            "workload": "held-out channel cases of the warm-start sweep (seed 2000, n <= %d), first-order AUSM, "
+                        "5-stage RK, CFL 1.5; plain = FP64 drop-in path case after case (e3d_solve, check every 50)"
+                        % n_max}
 
 
 def run_sweep_workload(a, rank, world):
@@ -396,7 +435,7 @@ def run_sweep_workload(a, rank, world):
             t0 = time.time()
             tr_specs = sw.polar_specs(1000, 24 if small else 200, n_range=nr, prefix="train")
             te_specs = sw.polar_specs(2000, 8 if small else 32, n_range=nr, prefix="test")
-            decks = sw.write_cases(td, tr_specs + te_specs, WARM_SCHEME, sides="channel")
+            decks = sw.write_cases(td, tr_specs + te_specs, sw.WARM_SCHEME, sides="channel")
             cases = [api.Case(d) for d in decks]
             train, test = cases[:len(tr_specs)], cases[len(tr_specs):]
             log(f"[bench] {len(cases)} cases written and loaded in {time.time() - t0:.1f}s")
@@ -461,6 +500,8 @@ def main():
                     help="device order of each block's real cells (e3d_options.renumber)")
     ap.add_argument("--no-error-report", action="store_true",
                     help="channel, fp32: skip the FP32-vs-FP64 error report (profiling runs)")
+    ap.add_argument("--warm-cases", type=int, default=4,
+                    help="channel: held-out cases of the bounded time-to-8-orders comparison (0: skip)")
     ap.add_argument("--fp64-steps", type=int, default=50,
                     help="channel, fp32: also time this many steps of the FP64 bitwise drop-in path (0: skip)")
     a = ap.parse_args()
@@ -598,6 +639,10 @@ def main():
                          "kernels_gbs": {k["name"]: (k["bytes_per_launch"] / (k["total_ms"] / k["launches"] / 1000.0)
                                                      / 1e9) if k["bytes_per_launch"] else None for k in kt64}}
             s64.close()
+        warm8 = None
+        if rank == 0 and world == 1 and a.workload == "channel" and a.warm_cases > 0:
+            s.close()  # frees the workload's device memory before the sweep
+            warm8 = warmstart_bounded(a.warm_cases)
         fp32_err = None
         if rank == 0 and a.precision == "fp32" and a.workload == "channel" and not a.no_error_report:
             fp32_err = fp32_error_report(td)
@@ -616,7 +661,7 @@ def main():
             "clocks": cl,
             "final": {"iterations": int(len(hist["iter"])), "ro_conv": float(hist["conv"][-1, 0]),
                       "cl": float(hist["cl"][-1]), "cd": float(hist["cd"][-1])},
-            "fp32_vs_fp64": fp32_err, "fp64_path": fp64_path}
+            "fp32_vs_fp64": fp32_err, "fp64_path": fp64_path, "time_to_8_orders": warm8}
     if rank == 0:
         print(json.dumps(line))
     s.close()

@@ -12,6 +12,8 @@ iteration), so both reach the same converged Cl/Cd.
 """
 from __future__ import annotations
 
+import argparse
+import json
 import multiprocessing as mp
 import os
 import time
@@ -156,3 +158,57 @@ def train_surrogate(cases: list[api.Case], seed: int, criterion: float = -4.0, m
     t_train = time.perf_counter() - t0
     return m, dict(samples=m.n_samples, solve_s=t_solve, train_s=t_train, loss=loss,
                    loss_first=float(np.mean(hist[:20])), cell_iters=cell_iters)
+
+
+def save_surrogate(m: api.Surrogate, path: str, info: dict) -> None:
+    """Trained parameters and input/output normalisation, with how they were made."""
+    params, norm = m.get_params()
+    np.savez_compressed(path, params=params, norm=norm, info=np.array(json.dumps(info)))
+
+
+def load_surrogate(path: str, gamma: float = 1.4, device: int = -1) -> tuple[api.Surrogate, dict]:
+    z = np.load(path)
+    m = api.Surrogate(seed=0, gamma=gamma, device=device)
+    m.set_params(z["params"], z["norm"])
+    return m, json.loads(str(z["info"]))
+
+
+# The warm-start workload: first-order AUSM on the channel variant of the bump
+# mesh (z planes and top SYMMETRY, inlet and outlet FARFIELD), where every case
+# of the sweep's Mach/alpha range converges to an 8-order drop.
+WARM_SCHEME = dict(order=1, flux="ausm", stages=5, cfl=1.5)
+TRAIN_SEED, HELD_OUT_SEED = 1000, 2000
+
+
+def train_warmstart(out: str, n_cases: int = 200, n_range=(25, 60), steps: int = 40000,
+                    workdir: str | None = None) -> dict:
+    """Solves the seeded training sweep, trains the surrogate on the converged
+    states and writes it to `out` (see save_surrogate)."""
+    import tempfile
+
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        specs = polar_specs(TRAIN_SEED, n_cases, n_range=n_range, prefix="train")
+        decks = write_cases(td, specs, WARM_SCHEME, sides="channel")
+        cases = [api.Case(d) for d in decks]
+        m, info = train_surrogate(cases, seed=TRAIN_SEED, criterion=-4.0, steps=steps)
+        info.update(scheme=WARM_SCHEME, train_seed=TRAIN_SEED, cases=n_cases, n_range=list(n_range))
+        save_surrogate(m, out, info)
+        for c in cases:
+            c.close()
+    return info
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description="Train the warm-start surrogate on the seeded channel sweep.")
+    ap.add_argument("command", choices=["train"])
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--cases", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=40000)
+    a = ap.parse_args(argv)
+    info = train_warmstart(a.out, n_cases=a.cases, steps=a.steps)
+    print(json.dumps(info))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
