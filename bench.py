@@ -433,14 +433,19 @@ def run_sweep_workload(a, rank, world):
                     "clocks": ClockSampler.summarize(clocks.stop())}
         else:
             t0 = time.time()
-            tr_specs = sw.polar_specs(1000, 24 if small else 200, n_range=nr, prefix="train")
+            need_train = a.retrain or small or not os.path.exists(WARM_DATA)
+            tr_specs = sw.polar_specs(1000, 24 if small else 200, n_range=nr, prefix="train") if need_train else []
             te_specs = sw.polar_specs(2000, 8 if small else 32, n_range=nr, prefix="test")
             decks = sw.write_cases(td, tr_specs + te_specs, sw.WARM_SCHEME, sides="channel")
             cases = [api.Case(d) for d in decks]
             train, test = cases[:len(tr_specs)], cases[len(tr_specs):]
             log(f"[bench] {len(cases)} cases written and loaded in {time.time() - t0:.1f}s")
             crit, max_iter = -8.0, 200000
-            m, tinfo = sw.train_surrogate(train, seed=1000, criterion=-4.0, steps=40000 if not small else 5000)
+            if need_train:
+                m, tinfo = sw.train_surrogate(train, seed=1000, criterion=-4.0, steps=40000 if not small else 5000)
+            else:  # the surrogate trained on the same 200 cases, committed (python -m euler3d_b200.sweep train)
+                m, tinfo = sw.load_surrogate(WARM_DATA)
+                tinfo = dict(tinfo, source=os.path.relpath(WARM_DATA, HERE))
             log(f"[bench] surrogate: {tinfo}")
             clocks.mark("start")
             learned = sw.solve_batched(test, crit, max_iter, surrogate=m)
@@ -500,6 +505,9 @@ def main():
                     help="device order of each block's real cells (e3d_options.renumber)")
     ap.add_argument("--no-error-report", action="store_true",
                     help="channel, fp32: skip the FP32-vs-FP64 error report (profiling runs)")
+    ap.add_argument("--retrain", action="store_true",
+                    help="warmstart: solve the 200 training cases and train the surrogate again instead of "
+                         "loading the committed one")
     ap.add_argument("--warm-cases", type=int, default=4,
                     help="channel: held-out cases of the bounded time-to-8-orders comparison (0: skip)")
     ap.add_argument("--fp64-steps", type=int, default=50,
