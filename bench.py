@@ -38,7 +38,7 @@ UNIT = "cell-iterations/s"
 WORKLOAD = dict(n=80, blocks=16, order=2, flux="roe", gradient="leastsquares", limiter="venkatakrishnan", k=5.0,
                 omega=2.16e-16, mach=0.7, aoa_deg=1.25, cfl=1.5, stages=5)
 REFDRIVER = os.path.join(HERE, "oracle", "_ref", "e3d_refdriver")
-RENUMBER = "none"  # device cell order of the channel workload (e3d_options.renumber)
+RENUMBER = "none+boundary_last"  # device cell order of the channel workload (the library's default)
 # the warm-start surrogate trained on the seeded channel sweep (python -m euler3d_b200.sweep train --out ...)
 WARM_DATA = os.path.join(HERE, "euler3d_b200", "data", "warmstart_channel_ausm1.npz")
 
@@ -501,7 +501,8 @@ def main():
                          "into a temporary directory when absent")
     ap.add_argument("--scale", choices=["full", "small"], default="full",
                     help="small: the same sweep workloads on 10^3..16^3 meshes (quick checks)")
-    ap.add_argument("--renumber", choices=["none", "rcm", "morton", "shuffle"], default=RENUMBER,
+    ap.add_argument("--renumber", default=RENUMBER,
+                    choices=[f"{b}{s}" for b in ("none", "rcm", "morton", "shuffle") for s in ("", "+boundary_last")],
                     help="device order of each block's real cells (e3d_options.renumber)")
     ap.add_argument("--no-error-report", action="store_true",
                     help="channel, fp32: skip the FP32-vs-FP64 error report (profiling runs)")

@@ -81,7 +81,8 @@ class Solver:
     """Device-resident solver over every block of a case."""
 
     def __init__(self, case: Case, precision: str = "fp64", carry_w0: int = -1, use_graph: bool = True,
-                 device: int = -1, stream: int | None = None, hist_capacity: int = 4096, renumber: str = "none"):
+                 device: int = -1, stream: int | None = None, hist_capacity: int = 4096,
+                 renumber: str = "none+boundary_last"):
         lib = L.lib()
         o = L.Options()
         lib.e3d_default_options(C.byref(o))
@@ -215,7 +216,7 @@ class Batch(Solver):
     """Several cases advanced together (one device arena, persistent kernel)."""
 
     def __init__(self, cases: list, precision: str = "fp32", use_graph: bool = True, device: int = -1,
-                 hist_capacity: int = 4096, renumber: str = "none"):
+                 hist_capacity: int = 4096, renumber: str = "none+boundary_last"):
         lib = L.lib()
         o = L.Options()
         lib.e3d_default_options(C.byref(o))

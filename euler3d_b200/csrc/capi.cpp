@@ -71,7 +71,7 @@ void e3d_default_options(e3d_options* o) {
 	o->device = -1;
 	o->stream = nullptr;
 	o->hist_capacity = 4096;
-	o->renumber = E3D_RENUMBER_NONE;
+	o->renumber = E3D_RENUMBER_NONE | E3D_RENUMBER_BOUNDARY_LAST;
 }
 
 int e3d_case_load(const char* deck_path, const char* workdir, e3d_case** out) {

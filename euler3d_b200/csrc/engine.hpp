@@ -21,13 +21,19 @@ struct EngineOptions {
 	int device = -1;     // -1: current device
 	cudaStream_t stream = nullptr;  // nullptr: the engine creates its own stream
 	size_t hist_capacity = 4096;    // iterations of per-block norm/force history kept on device
-	int renumber = 0;    // RENUMBER_*: device order of each block's real cells
+	int renumber = 16;   // RENUMBER_*: device order of each block's real cells (file order, boundary cells last)
 };
 
 // Device order of the real cells inside each block (renumber.cpp).  Slots keep
 // each cell's ascending face order, so every per-cell sum runs in the
 // reference's order whatever the cell order.
-enum Renumber : int { RENUMBER_NONE = 0, RENUMBER_RCM = 1, RENUMBER_MORTON = 2, RENUMBER_SHUFFLE = 3 };
+enum Renumber : int {
+	RENUMBER_NONE = 0,
+	RENUMBER_RCM = 1,
+	RENUMBER_MORTON = 2,
+	RENUMBER_SHUFFLE = 3,
+	RENUMBER_BOUNDARY_LAST = 16  // added to a base order: cells with a ghost neighbour last
+};
 // order[i] = block-local real cell placed i-th on the device
 std::vector<int> cell_order(const HostBlock& b, int mode);
 

@@ -16,6 +16,14 @@
 //                     block's bounding box, one scale for all three axes)
 //   RENUMBER_SHUFFLE  a seeded random order: the worst case, for tests and
 //                     measurement
+//
+// RENUMBER_BOUNDARY_LAST, added to any of these, then moves the cells that
+// have a ghost neighbour (a boundary or connexion face) to the end of the
+// block, each group keeping the base order.  The stage passes do extra work
+// for such a cell (the ghost's reflected gradient, limiter and face state;
+// its boundary condition); a warp runs that work if any of its 32 cells needs
+// it, and in file order nearly every warp holds one.  Grouped, only the
+// boundary cells' warps run it.
 #include <algorithm>
 #include <cstdint>
 #include <numeric>
@@ -159,9 +167,8 @@ std::vector<int> shuffled(const HostBlock& b) {
 	return order;
 }
 
-}  // namespace
 
-std::vector<int> cell_order(const HostBlock& b, int mode) {
+std::vector<int> base_order(const HostBlock& b, int mode) {
 	switch (mode) {
 	case RENUMBER_NONE: {
 		std::vector<int> order(b.n_real);
@@ -173,6 +180,22 @@ std::vector<int> cell_order(const HostBlock& b, int mode) {
 	case RENUMBER_SHUFFLE: return shuffled(b);
 	default: throw Error(E3D_ERR_ARG, "unknown cell renumbering " + std::to_string(mode));
 	}
+}
+
+}  // namespace
+
+std::vector<int> cell_order(const HostBlock& b, int mode) {
+	if (mode < 0 || (mode & ~(RENUMBER_BOUNDARY_LAST | 15)) != 0)
+		throw Error(E3D_ERR_ARG, "unknown cell renumbering " + std::to_string(mode));
+	std::vector<int> order = base_order(b, mode & 15);
+	if (mode & RENUMBER_BOUNDARY_LAST) {
+		std::vector<char> boundary(b.n_real, 0);
+		for (int c = 0; c < b.n_real; c++)
+			for (int j = b.cell_face_ptr[c]; j < b.cell_face_ptr[c + 1]; j++)
+				if (b.cell_cells[j] >= b.n_real) boundary[c] = 1;
+		std::stable_partition(order.begin(), order.end(), [&](int c) { return !boundary[c]; });
+	}
+	return order;
 }
 
 }  // namespace e3d

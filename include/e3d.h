@@ -57,16 +57,21 @@ typedef struct e3d_block_info {
 	int n_real, n_all, n_faces, n_nodes, n_markers, n_real_boundaries, n_wall_faces;
 } e3d_block_info;
 
-/* device order of each block's real cells (e3d_options.renumber).  No
- * counterpart in the reference, which keeps file order.  A cell's slots keep
- * its ascending face order, so FP64 results are bit for bit the same in every
- * order; state transfers (e3d_state_get/set) stay in file order.  The state
- * blob of e3d_state_export and the rows of e3d_cell_features are in device
- * order. */
+/* device order of each block's real cells (e3d_options.renumber; by default
+ * file order with the cells that have a ghost neighbour moved to the end of
+ * their block).  No counterpart in the reference, which keeps file order.  A
+ * cell's slots keep its ascending face order, so FP64 results are bit for bit
+ * the same in every order; state transfers (e3d_state_get/set) stay in file
+ * order.  The state blob of e3d_state_export and the rows of
+ * e3d_cell_features are in device order. */
 #define E3D_RENUMBER_NONE 0    /* file order */
 #define E3D_RENUMBER_RCM 1     /* reverse Cuthill-McKee on the cell adjacency graph */
 #define E3D_RENUMBER_MORTON 2  /* Z-order curve of the cell centres */
 #define E3D_RENUMBER_SHUFFLE 3 /* seeded random order (worst case, for tests and measurement) */
+/* added to any of the above: the cells with a ghost neighbour (boundary and
+ * connexion faces) move to the end of their block, each group in the base
+ * order, so that the stage passes' extra work for them runs in their warps only */
+#define E3D_RENUMBER_BOUNDARY_LAST 16
 
 typedef struct e3d_options {
 	int precision;    /* E3D_FP64 or E3D_FP32 */
@@ -75,7 +80,7 @@ typedef struct e3d_options {
 	int device;       /* -1: current device */
 	void* stream;     /* cudaStream_t or NULL (solver creates its own) */
 	int hist_capacity;/* iterations of history buffered on the device (0: 4096) */
-	int renumber;     /* E3D_RENUMBER_* (default E3D_RENUMBER_NONE) */
+	int renumber;     /* E3D_RENUMBER_* (default E3D_RENUMBER_NONE | E3D_RENUMBER_BOUNDARY_LAST) */
 } e3d_options;
 
 /* One outer iteration's post-processing (PostProcessing::process,

@@ -112,7 +112,7 @@ def test_fused_fp64_matches_reference(name, tmp_path):
     assert np.max(np.abs(h["conv"][:, 0] - g.hist("ro_conv"))) < 1e-11
 
 
-@pytest.mark.parametrize("renumber", ["rcm", "morton", "shuffle"])
+@pytest.mark.parametrize("renumber", ["none", "rcm", "morton", "shuffle", "morton+boundary_last"])
 @pytest.mark.parametrize("name", golden_names())
 def test_fused_fp64_any_cell_order(name, renumber, tmp_path):
     """Renumbering moves where a cell's data sits on the device, not the order

@@ -86,7 +86,7 @@ def test_fused_fp64_on_reference_meshes(name, tmp_path):
         assert np.array_equal(h[col], g.hist(col)), col
 
 
-@pytest.mark.parametrize("renumber", ["rcm", "morton"])
+@pytest.mark.parametrize("renumber", ["none", "rcm", "morton"])
 @pytest.mark.parametrize("name", ["ref_naca_o2_gg_bj_ausm", "ref_onera_o2_ls_venk_roe"])
 def test_fused_fp64_renumbered_on_reference_meshes(name, renumber, tmp_path):
     """Renumbered device order on the reference's meshes: the same arrays."""

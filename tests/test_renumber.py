@@ -24,7 +24,7 @@ def _bandwidth(case, b, order):
     return int(np.max(np.abs(pos[own[keep]] - pos[other[keep]])))
 
 
-@pytest.mark.parametrize("mode", ["none", "rcm", "morton", "shuffle"])
+@pytest.mark.parametrize("mode", ["none", "rcm", "morton", "shuffle", "none+boundary_last", "morton+boundary_last"])
 def test_orders_are_permutations(mode, tmp_path):
     case = Case(mg.write_case(str(tmp_path), 6, 2))
     for b in range(case.n_blocks):
@@ -34,6 +34,26 @@ def test_orders_are_permutations(mode, tmp_path):
             assert np.array_equal(o, np.arange(o.size))
     # deterministic
     assert np.array_equal(case.cell_order(1, mode), case.cell_order(1, mode))
+
+
+@pytest.mark.parametrize("base", ["none", "morton"])
+def test_boundary_last_groups_cells_with_ghost_neighbours(base, tmp_path):
+    """Cells with a ghost neighbour (boundary or connexion face) come last in
+    their block; each group keeps the base order."""
+    case = Case(mg.write_case(str(tmp_path), 6, 3))
+    for b in range(case.n_blocks):
+        n = case.block_info(b).n_real
+        ptr = case.get(b, "cell_face_ptr")
+        nbr = case.get(b, "cell_cells")
+        own = np.repeat(np.arange(n), np.diff(ptr[:n + 1]))
+        boundary = np.zeros(n, bool)
+        boundary[own[nbr[:ptr[n]] >= n]] = True
+        o = case.cell_order(b, base + "+boundary_last")
+        k = int(np.count_nonzero(~boundary))
+        assert 0 < k < n
+        assert not boundary[o[:k]].any() and boundary[o[k:]].all()
+        ref = case.cell_order(b, base)
+        assert np.array_equal(o[:k], ref[~boundary[ref]]) and np.array_equal(o[k:], ref[boundary[ref]])
 
 
 def test_rcm_restores_locality_of_a_shuffled_order(tmp_path):
