@@ -17,6 +17,9 @@ A step is one outer iteration of the solver over every cell of every block
 
 N > 1 runs N independent replicas (one per GPU, launched by torchrun): the
 path has no inter-GPU exchange when all blocks of a case live on one GPU.
+``--mode blocks`` instead splits the one case's 16 blocks over the N ranks
+(the reference's MPI distribution; the connexion halo crosses GPUs through
+NCCL once per outer iteration) and reports strong scaling.
 """
 from __future__ import annotations
 
@@ -481,6 +484,116 @@ def run_sweep_workload(a, rank, world):
     return 0
 
 
+def run_block_sharded(a, rank: int, world: int, local: int) -> int:
+    """The channel case with its blocks split over the ranks (euler3d_b200.shard):
+    every rank advances its block range, the connexion halo crosses ranks
+    after every outer iteration (NCCL all-to-all on the solver stream; no
+    exchange at N = 1), and the job's time is the slowest rank's device time
+    over the K iterations (CUDA events on the solver stream)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from euler3d_b200 import _lib as L
+    from euler3d_b200 import shard
+    from euler3d_b200.api import Case
+
+    torch.cuda.set_device(local)
+    timeout = datetime.timedelta(seconds=120)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", local))
+    else:
+        import socket
+
+        so = socket.socket()
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+        so.close()
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                timeout=timeout)
+    warm, steps = max(3, a.warmup), max(1, a.steps)
+    with tempfile.TemporaryDirectory() as td:
+        case = Case(make_case(td, a.n, a.blocks))
+        cfg = workload_config(a.n, a.blocks, a.precision)
+        cfg["cell_order"] = a.renumber
+        run = shard.Sharded(case, precision=a.precision, device=local, renumber=a.renumber,
+                            hist_capacity=max(4096, steps + warm + 64))
+        s = run.solver
+        cells_all = sum(case.block_info(b).n_real for b in range(case.n_blocks))
+        cells_mine = sum(info.n_real for info in s._info)
+        clocks = ClockSampler(local)
+        run.iterate(warm)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks.mark("start")
+        e0.record(run.stream)
+        run.step(steps)
+        e1.record(run.stream)
+        e1.synchronize()
+        clocks.mark("end")
+        run.gather()
+        ms_t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64)
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX, group=run.ctrl)
+        ms = float(ms_t.item())
+        hist = run.history()
+        assert all(abs(x) < 1e300 for x in hist["rms"][:, 0]), "non-finite residual"
+        halo = int(s.send_counts.sum() + s.recv_counts.sum())
+        launches = (s.launches_per_iteration() + 2) * steps
+        # end to end through the public API with host buffers: every step
+        # imports this rank's solver state from pinned host memory, runs one
+        # sharded iteration (halo exchange and norm gather included) and
+        # exports the state back
+        nbytes = s.state_bytes()
+        host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        lib = L.lib()
+        L.check(lib.e3d_state_export(s._h, C.c_void_p(host.data_ptr()), nbytes))
+        e2e_steps = max(3, a.e2e_steps)
+        dist.barrier()
+        te = time.perf_counter()
+        for _ in range(e2e_steps):
+            L.check(lib.e3d_state_import(s._h, C.c_void_p(host.data_ptr()), nbytes))
+            run.iterate(1)
+            L.check(lib.e3d_state_export(s._h, C.c_void_p(host.data_ptr()), nbytes))
+        te_t = torch.tensor([time.perf_counter() - te], dtype=torch.float64)
+        dist.all_reduce(te_t, op=dist.ReduceOp.MAX, group=run.ctrl)
+        e2e = {"value": cells_all * e2e_steps / float(te_t.item()), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": e2e_steps,
+               "path": "e3d_state_import (pinned host) + one sharded iteration (halo exchange, norm gather) + "
+                       "e3d_state_export, host wall clock, max over ranks"}
+        kt = s.time_kernels(min(steps, 10))
+        dom = max((k for k in kt if k["bytes_per_launch"]), key=lambda k: k["total_ms"])
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = dom["bytes_per_launch"] / (dom["total_ms"] / dom["launches"] / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "kernel": dom["name"],
+                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                    "note": "rank 0's blocks"}
+        cl = ClockSampler.summarize(clocks.stop())
+        line = {"metric": METRIC, "value": cells_all * steps / (ms / 1000.0), "unit": UNIT, "n_gpus": world,
+                "steps": steps, "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32" if a.precision == "fp32" else "f64",
+                "data": "synthetic", "config": dict(cfg, parallelism=f"blocks{world}", cells=cells_all,
+                                                    rank0_cells=cells_mine, rank0_halo_entries=halo,
+                                                    transport=run.transport),
+                "roofline": roofline, "cpu_baseline": None, "e2e": e2e, "gpu_launches": launches, "clocks": cl,
+                "final": {"iterations": int(len(hist["iter"])), "ro_conv": float(hist["conv"][-1, 0]),
+                          "cl": float(hist["cl"][-1]), "cd": float(hist["cd"][-1])}}
+        if rank == 0:
+            print(json.dumps(line))
+        run.close()
+        case.close()
+    dist.barrier(group=None)
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -513,6 +626,9 @@ def main():
                     help="channel: held-out cases of the bounded time-to-8-orders comparison (0: skip)")
     ap.add_argument("--fp64-steps", type=int, default=50,
                     help="channel, fp32: also time this many steps of the FP64 bitwise drop-in path (0: skip)")
+    ap.add_argument("--mode", choices=["replicas", "blocks"], default="replicas",
+                    help="channel, N GPUs: N independent copies of the case (weak scaling, default), or the case's "
+                         "blocks split over the N ranks with the halo exchanged every iteration (strong scaling)")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -521,6 +637,8 @@ def main():
         return run_reference_arm(a, rank)
     if a.workload not in ("channel", "wing"):
         return run_sweep_workload(a, rank, world)
+    if a.mode == "blocks":
+        return run_block_sharded(a, rank, world, local)
 
     import torch
     import torch.distributed as dist

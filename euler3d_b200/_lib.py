@@ -124,6 +124,16 @@ SIGNATURES = {
     "e3d_surrogate_get_params": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "e3d_surrogate_set_params": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "e3d_warm_start": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "e3d_shard_first_blocks": ([C.c_int, C.c_int, C.c_void_p], C.c_int),
+    "e3d_case_shard_plan": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_void_p], C.c_int),
+    "e3d_shard_create": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(Options), C.POINTER(C.c_void_p)],
+                         C.c_int),
+    "e3d_shard_halo_counts": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "e3d_shard_pack": ([C.c_void_p, C.c_void_p], C.c_int),
+    "e3d_shard_unpack": ([C.c_void_p, C.c_void_p], C.c_int),
+    "e3d_shard_flow_data": ([C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int)], C.c_int),
+    "e3d_shard_push_flow_data": ([C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "e3d_residual_norms_noalloc": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                     C.c_void_p], C.c_int),
 }

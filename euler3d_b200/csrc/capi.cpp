@@ -200,30 +200,119 @@ int e3d_case_get_i32(const e3d_case* c, int block, const char* name, int32_t* ds
 	});
 }
 
+static e3d::EngineOptions engine_options(const e3d_options* opt) {
+	e3d_options o;
+	e3d_default_options(&o);
+	if (opt) o = *opt;
+	e3d::EngineOptions eo;
+	eo.precision = o.precision;
+	eo.carry_w0 = o.carry_w0;
+	eo.use_graph = o.use_graph;
+	eo.device = o.device;
+	eo.stream = static_cast<cudaStream_t>(o.stream);
+	eo.hist_capacity = o.hist_capacity > 0 ? (size_t)o.hist_capacity : 4096;
+	eo.renumber = o.renumber;
+	return eo;
+}
+
 int e3d_solver_create(const e3d_case* c, const e3d_options* opt, e3d_solver** out) {
 	if (!c || !out) return fail(E3D_ERR_ARG, "null argument");
 	*out = nullptr;
 	return guard([&] {
-		e3d_options o;
-		e3d_default_options(&o);
-		if (opt) o = *opt;
-		e3d::EngineOptions eo;
-		eo.precision = o.precision;
-		eo.carry_w0 = o.carry_w0;
-		eo.use_graph = o.use_graph;
-		eo.device = o.device;
-		eo.stream = static_cast<cudaStream_t>(o.stream);
-		eo.hist_capacity = o.hist_capacity > 0 ? (size_t)o.hist_capacity : 4096;
-		eo.renumber = o.renumber;
-		auto* s = new e3d_solver;
-		try {
-			s->eng.reset(new e3d::Engine(c->hc, eo));
-		} catch (...) {
-			delete s;
-			throw;
-		}
-		*out = s;
+		const e3d::EngineOptions eo = engine_options(opt);
+		auto s = std::make_unique<e3d_solver>();
+		s->eng.reset(new e3d::Engine(c->hc, eo));
+		*out = s.release();
 	});
+}
+
+// ---- block sharding
+static std::vector<int> first_blocks(const e3d_case* c, const int32_t* first_block, int n_ranks) {
+	if (!c || !first_block) throw e3d::Error(E3D_ERR_ARG, "null argument");
+	if (n_ranks < 1) throw e3d::Error(E3D_ERR_ARG, "sharding: at least one rank");
+	return std::vector<int>(first_block, first_block + n_ranks + 1);
+}
+
+int e3d_shard_first_blocks(int n_blocks, int n_ranks, int32_t* first_block) {
+	if (!first_block) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		const std::vector<int> f = e3d::shard_first_blocks(n_blocks, n_ranks);
+		std::copy(f.begin(), f.end(), first_block);
+	});
+}
+
+int e3d_case_shard_plan(const e3d_case* c, const int32_t* first_block, int n_ranks, int rank, int64_t* send_counts,
+                        int64_t* recv_counts, int32_t* send_cells, int32_t* recv_cells) {
+	if (!send_counts || !recv_counts) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		const e3d::ShardPlan p = e3d::shard_plan(c->hc, first_blocks(c, first_block, n_ranks), rank);
+		for (int r = 0; r < n_ranks; r++) {
+			send_counts[r] = p.send_count[r];
+			recv_counts[r] = p.recv_count[r];
+		}
+		if (send_cells)
+			for (size_t i = 0; i < p.send_cell.size(); i++) {
+				send_cells[2 * i] = p.send_block[i];
+				send_cells[2 * i + 1] = p.send_cell[i];
+			}
+		if (recv_cells)
+			for (size_t i = 0; i < p.recv_cell.size(); i++) {
+				recv_cells[2 * i] = p.recv_block[i];
+				recv_cells[2 * i + 1] = p.recv_cell[i];
+			}
+	});
+}
+
+int e3d_shard_create(const e3d_case* c, const int32_t* first_block, int n_ranks, int rank, const e3d_options* opt,
+                     e3d_solver** out) {
+	if (!c || !out) return fail(E3D_ERR_ARG, "null argument");
+	*out = nullptr;
+	return guard([&] {
+		const e3d::ShardPlan p = e3d::shard_plan(c->hc, first_blocks(c, first_block, n_ranks), rank);
+		const e3d::EngineOptions eo = engine_options(opt);
+		auto s = std::make_unique<e3d_solver>();
+		s->eng.reset(new e3d::Engine(c->hc, eo, p));
+		*out = s.release();
+	});
+}
+
+static e3d::Engine& shard(e3d_solver* s) {
+	e3d::Engine& e = eng(s);
+	if (!e.is_shard()) throw e3d::Error(E3D_ERR_STATE, "not a shard solver (e3d_shard_create)");
+	return e;
+}
+
+int e3d_shard_halo_counts(const e3d_solver* s, int64_t* send_counts, int64_t* recv_counts) {
+	if (!send_counts || !recv_counts) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		const e3d::ShardPlan& p = shard(const_cast<e3d_solver*>(s)).shard();
+		for (int r = 0; r < p.n_ranks; r++) {
+			send_counts[r] = p.send_count[r];
+			recv_counts[r] = p.recv_count[r];
+		}
+	});
+}
+
+int e3d_shard_pack(e3d_solver* s, void* send) { return guard([&] { shard(s).shard_pack(send); }); }
+
+int e3d_shard_unpack(e3d_solver* s, const void* recv) { return guard([&] { shard(s).shard_unpack(recv); }); }
+
+int e3d_shard_flow_data(e3d_solver* s, double* out, int64_t capacity, int* n_iters) {
+	if (!n_iters) return fail(E3D_ERR_ARG, "null argument");
+	return guard([&] {
+		e3d::Engine& e = shard(s);
+		const int n = e.shard_pending();
+		*n_iters = n;
+		if (!out) return;
+		if (capacity < (int64_t)n * e.n_blocks() * 10) throw e3d::Error(E3D_ERR_ARG, "flow data: buffer too small");
+		int m = 0;
+		const std::vector<double> v = e.shard_take_flow_data(m);
+		std::copy(v.begin(), v.end(), out);
+	});
+}
+
+int e3d_shard_push_flow_data(e3d_solver* s, const double* all_blocks, int n_iters) {
+	return guard([&] { shard(s).shard_push(all_blocks, n_iters); });
 }
 
 int e3d_batch_create(const e3d_case* const* cases, int n_cases, const e3d_options* opt, e3d_solver** out) {

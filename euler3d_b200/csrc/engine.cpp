@@ -70,7 +70,12 @@ static void rk_tables(int stages, std::vector<double>& a, std::vector<double>& b
 
 Engine::Engine(const HostCase& hc, const EngineOptions& opt) : Engine(std::vector<const HostCase*>{&hc}, opt) {}
 
-Engine::Engine(const std::vector<const HostCase*>& cases, const EngineOptions& opt)
+Engine::Engine(const HostCase& hc, const EngineOptions& opt, const ShardPlan& plan)
+    : Engine(std::vector<const HostCase*>{&hc}, opt, &plan) {}
+
+Engine::Engine(const std::vector<const HostCase*>& cases, const EngineOptions& opt) : Engine(cases, opt, nullptr) {}
+
+Engine::Engine(const std::vector<const HostCase*>& cases, const EngineOptions& opt, const ShardPlan* plan)
     : deck_(cases.empty() ? Deck() : cases[0]->deck), opt_(opt) {
 	if (cases.empty()) throw Error(E3D_ERR_ARG, "no case");
 	for (const HostCase* c : cases) {
@@ -139,15 +144,50 @@ Engine::Engine(const std::vector<const HostCase*>& cases, const EngineOptions& o
 		cuda_ok(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
 		own_stream_ = true;
 	}
-	setup(cases);
+	setup(cases, plan);
 	init_state();
 }
 
-void Engine::setup(const std::vector<const HostCase*>& cases) {
-	HostCase merged;
+void Engine::setup(const std::vector<const HostCase*>& cases, const ShardPlan* plan) {
 	case_boff_.assign(1, 0);
 	std::vector<const HostBlock*> blocks;
 	std::vector<Connexion> conns;
+	if (plan) {
+		// one rank's range of a single case: its blocks renumbered from 0, the
+		// connexions inside the range kept as device copies
+		if (cases.size() != 1) throw Error(E3D_ERR_ARG, "a shard holds blocks of one case");
+		const HostCase& hc = *cases[0];
+		if (plan->b1 > (int)hc.blocks.size() || plan->b0 < 0 || plan->b0 >= plan->b1)
+			throw Error(E3D_ERR_ARG, "sharding: block range outside the case");
+		for (int b = plan->b0; b < plan->b1; b++) blocks.push_back(&hc.blocks[b]);
+		for (Connexion k : plan->local) {
+			k.dest_block -= plan->b0;
+			k.origin_block -= plan->b0;
+			conns.push_back(std::move(k));
+		}
+		case_boff_.push_back((int)blocks.size());
+		build_blocks(blocks, conns);
+		shard_ = true;
+		need_exchange_ = true;  // Solver.cpp:48: the halo runs before the first iteration
+		plan_ = *plan;
+		for (const HostBlock& B : hc.blocks) all_n_real_.push_back(B.n_real);
+		std::vector<int> xs(plan->send_cell.size()), xr(plan->recv_cell.size());
+		for (size_t i = 0; i < xs.size(); i++) {
+			const int b = plan->send_block[i] - plan->b0;
+			if (b < 0 || b >= nb_ || plan->send_cell[i] < 0 || plan->send_cell[i] >= n_all_b_[b])
+				throw Error(E3D_ERR_MESH, "sharding: sent halo cell outside its block");
+			xs[i] = device_cell(b, plan->send_cell[i]);
+		}
+		for (size_t i = 0; i < xr.size(); i++) {
+			const int b = plan->recv_block[i] - plan->b0;
+			if (b < 0 || b >= nb_ || plan->recv_cell[i] < n_real_b_[b] || plan->recv_cell[i] >= n_all_b_[b])
+				throw Error(E3D_ERR_MESH, "sharding: received halo entry is not a ghost cell of its block");
+			xr[i] = device_cell(b, plan->recv_cell[i]);
+		}
+		xsend_.upload(xs);
+		xrecv_.upload(xr);
+		return;
+	}
 	for (const HostCase* c : cases) {
 		const int off = (int)blocks.size();
 		for (const HostBlock& b : c->blocks) blocks.push_back(&b);
@@ -159,6 +199,10 @@ void Engine::setup(const std::vector<const HostCase*>& cases) {
 		case_boff_.push_back((int)blocks.size());
 	}
 	build_blocks(blocks, conns);
+}
+
+int Engine::device_cell(int b, int local) const {
+	return local < n_real_b_[b] ? roff_[b] + pos_[b][local] : NR_ + goff_[b] + (local - n_real_b_[b]);
 }
 
 long long Engine::n_real_case(int c) const {
@@ -445,7 +489,7 @@ void Engine::init_state() {
 void Engine::count_device_bytes() {
 	size_t bytes = 0;
 	for (auto* b : {&slot_ptr_, &slot_face_, &slot_nbr_, &slot_mate_, &face_lr_, &halo_dst_, &halo_src_, &wall_off_,
-	                &wall_face_, &roff_d_})
+	                &wall_face_, &roff_d_, &xsend_, &xrecv_})
 		bytes += b->n * sizeof(int);
 	for (auto* b : {&S_, &nhat_, &area_, &rl_, &rr_, &fc_, &vol64_, &lsw64_, &W0_, &srad_, &grad_, &lim_, &partial_,
 	                &hist_d_})
@@ -750,6 +794,7 @@ template <class T>
 void Engine::run_iterations(Fused<T>& f, int n) {
 	const int stages = (int)alpha_.size();
 	while (n > 0) {
+		if (dev_iter_ == (int)opt_.hist_capacity) collect_history(total_iter_, dev_iter_);
 		const int room = (int)opt_.hist_capacity - dev_iter_;
 		const int m = std::min(n, room);
 		for (int i = 0; i < m; i++) {
@@ -771,12 +816,23 @@ void Engine::run_iterations(Fused<T>& f, int n) {
 		}
 		dev_iter_ += m;
 		n -= m;
-		collect_history(total_iter_, dev_iter_);
+		// a shard's records need every rank's norms: kept on the device until taken
+		if (!shard_) collect_history(total_iter_, dev_iter_);
 	}
+	if (shard_) need_exchange_ = !plan_.recv_cell.empty() || !plan_.send_cell.empty();
+}
+
+void Engine::require_exchanged(int n_iter) const {
+	if (!shard_ || (plan_.recv_cell.empty() && plan_.send_cell.empty())) return;
+	if (n_iter > 1)
+		throw Error(E3D_ERR_ARG, "a shard advances one iteration at a time: its halo crosses ranks after each one");
+	if (n_iter == 1 && need_exchange_)
+		throw Error(E3D_ERR_STATE, "shard halo not exchanged: pack, move the buffers and unpack before iterating");
 }
 
 void Engine::iterate(int n) {
 	if (n < 0) throw Error(E3D_ERR_ARG, "negative iteration count");
+	require_exchanged(n);
 	if (!started_) halo();  // Solver.cpp:48, before the first iteration
 	if (opt_.precision == PREC_FP64) run_iterations(f64_, n);
 	else run_iterations(f32_, n);
@@ -784,6 +840,7 @@ void Engine::iterate(int n) {
 
 double Engine::iterate_timed(int n) {
 	if (n < 0) throw Error(E3D_ERR_ARG, "negative iteration count");
+	require_exchanged(n);
 	if (!started_) halo();
 	if ((int)opt_.hist_capacity - dev_iter_ < n) collect_history(total_iter_, dev_iter_);
 	if ((int)opt_.hist_capacity < n) throw Error(E3D_ERR_LIMIT, "timed run longer than the history capacity");
@@ -818,7 +875,8 @@ double Engine::iterate_timed(int n) {
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	dev_iter_ += n;
-	collect_history(total_iter_, dev_iter_);
+	if (shard_) need_exchange_ = !plan_.recv_cell.empty() || !plan_.send_cell.empty();
+	else collect_history(total_iter_, dev_iter_);
 	return (double)ms;
 }
 
@@ -887,8 +945,83 @@ void Engine::import_state(const void* host, size_t bytes) {
 	started_ = true;
 }
 
+// One whole-case record from the per-block norms and forces x[nblocks][10].
+IterRecord Engine::make_record(int cs, const double* x, int nblocks, const int* n_real) {
+	IterRecord r{};
+	r.iter = (int)hist_case_[cs].size();
+	const double aoa = case_aoa_[cs];
+	for (int b = 0; b < nblocks; b++, x += 10) {
+		const double N = (double)n_real[b];
+		// Convergence::calculate*Rms (Convergence.cpp:27-48) then the block sum
+		// (BlockCommunicator.cpp:342-369)
+		for (int q = 0; q < 5; q++) r.rms[q] += (1. / N) * std::pow(x[q], 0.5);
+		// AerodynamicParameters::calculateGlobalCl/Cd (AerodynamicParameters.cpp:114-138)
+		const double cl_ = x[5], cd_ = x[6];
+		r.cl += cl_ * std::cos(aoa) - cd_ * std::sin(aoa);
+		r.cd += cl_ * std::sin(aoa) + cd_ * std::cos(aoa);
+		r.cmx += x[7];
+		r.cmy += x[8];
+		r.cmz += x[9];
+	}
+	if (!have_rms0_[cs]) {
+		for (int q = 0; q < 5; q++) rms0_[cs][q] = r.rms[q];
+		have_rms0_[cs] = 1;
+	}
+	for (int q = 0; q < 5; q++) r.conv[q] = std::log10(r.rms[q]) - std::log10(rms0_[cs][q]);
+	return r;
+}
+
+void Engine::shard_pack(void* send) {
+	if (!shard_) throw Error(E3D_ERR_STATE, "not a shard");
+	const int n = (int)xsend_.n;
+	if (n && !send) throw Error(E3D_ERR_ARG, "null send buffer");
+	if (opt_.precision == PREC_FP64)
+		launch_halo_pack<double>(n, xsend_.p, NA_, cur_ ? f64_.P1.p : f64_.P0.p, static_cast<double*>(send), st_);
+	else
+		launch_halo_pack<float>(n, xsend_.p, NA_, cur_ ? f32_.P1.p : f32_.P0.p, static_cast<float*>(send), st_);
+	check("halo pack");
+}
+
+void Engine::shard_unpack(const void* recv) {
+	if (!shard_) throw Error(E3D_ERR_STATE, "not a shard");
+	const int n = (int)xrecv_.n;
+	if (n && !recv) throw Error(E3D_ERR_ARG, "null receive buffer");
+	if (opt_.precision == PREC_FP64)
+		launch_halo_unpack<double>(n, xrecv_.p, NA_, static_cast<const double*>(recv), cur_ ? f64_.P1.p : f64_.P0.p,
+		                           cur_ ? f64_.P0.p : f64_.P1.p, st_);
+	else
+		launch_halo_unpack<float>(n, xrecv_.p, NA_, static_cast<const float*>(recv), cur_ ? f32_.P1.p : f32_.P0.p,
+		                          cur_ ? f32_.P0.p : f32_.P1.p, st_);
+	check("halo unpack");
+	need_exchange_ = false;
+}
+
+int Engine::shard_pending() {
+	if (!shard_) throw Error(E3D_ERR_STATE, "not a shard");
+	collect_history(total_iter_, dev_iter_);
+	return raw_iters_;
+}
+
+std::vector<double> Engine::shard_take_flow_data(int& n_iters) {
+	shard_pending();
+	std::vector<double> out;
+	out.swap(raw_pending_);
+	n_iters = raw_iters_;
+	raw_iters_ = 0;
+	return out;
+}
+
+void Engine::shard_push(const double* all_blocks, int n_iters) {
+	if (!shard_) throw Error(E3D_ERR_STATE, "not a shard");
+	if (n_iters < 0 || (n_iters && !all_blocks)) throw Error(E3D_ERR_ARG, "flow data: bad arguments");
+	const int nb = (int)all_n_real_.size();
+	for (int i = 0; i < n_iters; i++)
+		hist_case_[0].push_back(make_record(0, all_blocks + (size_t)i * nb * 10, nb, all_n_real_.data()));
+}
+
 // Pulls the device history records, converts them to the reference's mesh-level
-// quantities, and resets the device counter.
+// quantities (a shard keeps them raw until the caller has every rank's), and
+// resets the device counter.
 void Engine::collect_history(int first_iter, int n) {
 	if (n <= 0) return;
 	std::vector<double> h((size_t)n * nb_ * 10);
@@ -898,34 +1031,20 @@ void Engine::collect_history(int first_iter, int n) {
 	cuda_ok(cudaMemcpyAsync(&bad, bad_d_.p, sizeof(int), cudaMemcpyDeviceToHost, st_), "d2h");
 	cuda_ok(cudaStreamSynchronize(st_), "sync");
 	dev_iter_ = 0;
-	for (int i = 0; i < n; i++) {
+	if (shard_) {
+		raw_pending_.insert(raw_pending_.end(), h.begin(), h.end());
+		raw_iters_ += n;
+		total_iter_ += n;
+		if (bad) throw Error(E3D_ERR_NONFINITE, "non-finite residual norm by iteration " + std::to_string(total_iter_ - 1));
+		return;
+	}
+	for (int i = 0; i < n; i++)
 		for (int cs = 0; cs < ncases_; cs++) {
 			if (!case_active_[cs]) continue;
-			IterRecord r{};
-			r.iter = (int)hist_case_[cs].size();
-			const double aoa = case_aoa_[cs];
-			for (int b = case_boff_[cs]; b < case_boff_[cs + 1]; b++) {
-				const double* x = &h[((size_t)i * nb_ + b) * 10];
-				const double N = (double)(roff_[b + 1] - roff_[b]);
-				// Convergence::calculate*Rms (Convergence.cpp:27-48) then the block sum
-				// (BlockCommunicator.cpp:342-369)
-				for (int q = 0; q < 5; q++) r.rms[q] += (1. / N) * std::pow(x[q], 0.5);
-				// AerodynamicParameters::calculateGlobalCl/Cd (AerodynamicParameters.cpp:114-138)
-				const double cl_ = x[5], cd_ = x[6];
-				r.cl += cl_ * std::cos(aoa) - cd_ * std::sin(aoa);
-				r.cd += cl_ * std::sin(aoa) + cd_ * std::cos(aoa);
-				r.cmx += x[7];
-				r.cmy += x[8];
-				r.cmz += x[9];
-			}
-			if (!have_rms0_[cs]) {
-				for (int q = 0; q < 5; q++) rms0_[cs][q] = r.rms[q];
-				have_rms0_[cs] = 1;
-			}
-			for (int q = 0; q < 5; q++) r.conv[q] = std::log10(r.rms[q]) - std::log10(rms0_[cs][q]);
-			hist_case_[cs].push_back(r);
+			const int b0 = case_boff_[cs];
+			hist_case_[cs].push_back(make_record(cs, &h[((size_t)i * nb_ + b0) * 10], case_boff_[cs + 1] - b0,
+			                                     &n_real_b_[b0]));
 		}
-	}
 	total_iter_ += n;
 	if (bad && tolerate_nonfinite_) {
 		// a batch solve drops the cases whose residual turned non-finite and goes on
@@ -953,6 +1072,9 @@ void Engine::collect_history(int first_iter, int n) {
 }
 
 int Engine::solve(int max_iter, double criterion, int check_every) {
+	if (shard_)
+		throw Error(E3D_ERR_STATE, "a shard's stop test needs the norms of every rank: iterate, exchange and push "
+		                           "the gathered flow data instead");
 	if (check_every < 1) check_every = 1;
 	int done = 0;
 	while (true) {
@@ -1561,6 +1683,7 @@ void Engine::autotune(int iters) {
 
 double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch, int stall_window,
                            std::vector<int>& iters_done) {
+	if (shard_) throw Error(E3D_ERR_STATE, "batch solves run on a whole case, not on a shard");
 	if (iters_per_launch < 1) iters_per_launch = 1;
 	if (!started_) halo();
 	collect_history(total_iter_, dev_iter_);

@@ -37,6 +37,22 @@ enum Renumber : int {
 // order[i] = block-local real cell placed i-th on the device
 std::vector<int> cell_order(const HostBlock& b, int mode);
 
+// Block sharding (shard.cpp): rank r of n holds the case blocks
+// [first_block[r], first_block[r+1]).  Halo entries that cross ranks are
+// listed in transport order: by peer rank, then topology order, then cell pair.
+struct ShardPlan {
+	int rank = 0, n_ranks = 1, b0 = 0, b1 = 0;
+	std::vector<int> first_block;                   // n_ranks + 1
+	std::vector<long long> send_count, recv_count;  // halo entries per peer rank
+	std::vector<int> send_block, send_cell;         // origin (case block, block-local cell) of each sent entry
+	std::vector<int> recv_block, recv_cell;         // destination (case block, block-local ghost) of each received one
+	std::vector<Connexion> local;                   // connexions with both blocks on this rank (case block ids)
+};
+// the reference's distribution: n_blocks / n_ranks blocks each, one more for
+// the first n_blocks % n_ranks ranks (BlockCommunicator.cpp:29-38)
+std::vector<int> shard_first_blocks(int n_blocks, int n_ranks);
+ShardPlan shard_plan(const HostCase& hc, const std::vector<int>& first_block, int rank);
+
 // Host copy of one outer iteration's results (reference PostProcessing fields).
 struct IterRecord {
 	int iter;
@@ -66,6 +82,9 @@ public:
 	// share gamma, CFL, RK stages and the strategy choices, and may differ in
 	// mesh, Mach number, angle of attack and reference chord
 	Engine(const std::vector<const HostCase*>& cases, const EngineOptions& opt);
+	// one rank's blocks of a block-sharded case (plan from shard_plan); block
+	// indices of the engine's methods are local to the rank's range
+	Engine(const HostCase& hc, const EngineOptions& opt, const ShardPlan& plan);
 	~Engine();
 	Engine(const Engine&) = delete;
 	Engine& operator=(const Engine&) = delete;
@@ -97,6 +116,24 @@ public:
 	void import_state(const void* host, size_t bytes);
 	// run until the reference stop test (max_iter or criterion) fires
 	int solve(int max_iter, double criterion, int check_every);
+
+	// --- block sharding: the halo entries that cross ranks.  After every
+	// iteration (and before the first) each rank packs what its peers need,
+	// the caller moves the buffers (an all-to-all with per-peer counts), and
+	// each rank unpacks what it received; a shard refuses to iterate until it
+	// has.  Buffers are device memory of 5 values per entry in the engine's
+	// precision, entry-major, in ShardPlan order; work is queued on stream().
+	bool is_shard() const { return shard_; }
+	const ShardPlan& shard() const { return plan_; }
+	void shard_pack(void* send);
+	void shard_unpack(const void* recv);
+	// raw per-block norms and forces ([n][local blocks][10]) of the iterations
+	// run since the last call; the caller gathers every rank's, in block
+	// order, and pushes them back with shard_push (the history then holds
+	// whole-case records, summed in block order as one GPU sums them)
+	int shard_pending();  // brings the device records over; iterations waiting to be taken
+	std::vector<double> shard_take_flow_data(int& n_iters);
+	void shard_push(const double* all_blocks, int n_iters);
 
 	// --- batches: every active case advanced by the persistent cooperative
 	// kernel (FP32); a case stops (its tiles leave the work list) once its
@@ -167,7 +204,11 @@ private:
 		DevBuf<T> P0, P1, FS, Rc, Rd, dt, sgeo, sS, srv, lsw, vol;
 		FusedView<T> view(bool flip) const;
 	};
-	void setup(const std::vector<const HostCase*>& cases);
+	Engine(const std::vector<const HostCase*>& cases, const EngineOptions& opt, const ShardPlan* plan);
+	void setup(const std::vector<const HostCase*>& cases, const ShardPlan* plan);
+	int device_cell(int b, int local) const;
+	IterRecord make_record(int cs, const double* x, int nblocks, const int* n_real);
+	void require_exchanged(int n_iter) const;
 	void build_blocks(const std::vector<const HostBlock*>& blocks, const std::vector<Connexion>& conns);
 	void to_local(int b, std::vector<double>& a, int rows, int ld) const;
 	void to_device(int b, std::vector<double>& a, int rows, int ld) const;
@@ -227,6 +268,13 @@ private:
 	std::vector<char> have_rms0_;
 	std::vector<std::array<double, 5>> rms0_;
 	std::vector<std::vector<IterRecord>> hist_case_;
+	// block sharding
+	bool shard_ = false, need_exchange_ = false;
+	ShardPlan plan_;
+	std::vector<int> all_n_real_;   // real cells of every block of the case
+	DevBuf<int> xsend_, xrecv_;     // device cells of the sent / received halo entries
+	std::vector<double> raw_pending_;
+	int raw_iters_ = 0;
 	cudaGraphExec_t graph_[2] = {nullptr, nullptr};
 	// batch (persistent kernel) state
 	std::vector<char> case_active_, case_failed_;  // failed: residual turned non-finite in a batch solve

@@ -5,6 +5,8 @@
 namespace e3d {
 
 template void launch_halo<float>(int, const int*, const int*, int, float*, float*, cudaStream_t);
+template void launch_halo_pack<float>(int, const int*, int, const float*, float*, cudaStream_t);
+template void launch_halo_unpack<float>(int, const int*, int, const float*, float*, float*, cudaStream_t);
 template void launch_reduce<float>(const ReduceArgs&, const float*, const float*, const float*, cudaStream_t);
 template void launch_recon<float>(const FusedView<float>&, const Physics&, int, int, bool, int, cudaStream_t);
 template void launch_start<float>(const FusedView<float>&, const Physics&, int, cudaStream_t);

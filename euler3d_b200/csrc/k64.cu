@@ -65,6 +65,8 @@ void launch_smooth(const GeoView& g, const StateView& s, double* j1, int r0, int
 }
 
 template void launch_halo<double>(int, const int*, const int*, int, double*, double*, cudaStream_t);
+template void launch_halo_pack<double>(int, const int*, int, const double*, double*, cudaStream_t);
+template void launch_halo_unpack<double>(int, const int*, int, const double*, double*, double*, cudaStream_t);
 template void launch_reduce<double>(const ReduceArgs&, const double*, const double*, const double*, cudaStream_t);
 template void launch_recon<double>(const FusedView<double>&, const Physics&, int, int, bool, int, cudaStream_t);
 template void launch_start<double>(const FusedView<double>&, const Physics&, int, cudaStream_t);

@@ -374,6 +374,34 @@ __global__ void k_halo(int n, const int* __restrict__ dst, const int* __restrict
 	if (b1) st5(b1, NA, d, q);
 }
 
+// The halo of a block-sharded case, split at the transport: pack gathers the
+// primitives of the origin cells another process needs into an entry-major
+// buffer (buf[5*i + q], q = rho u v w p), unpack writes received entries into
+// the connexion ghosts of both state buffers, as k_halo does for local ones.
+template <class T>
+__global__ void k_halo_pack(int n, const int* __restrict__ src, int NA, const T* __restrict__ P,
+                            T* __restrict__ buf) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n) return;
+	const Q5<T> q = ld5(P, NA, src[t]);
+	T* o = buf + 5 * (size_t)t;
+	o[0] = q.r;
+	o[1] = q.u;
+	o[2] = q.v;
+	o[3] = q.w;
+	o[4] = q.p;
+}
+
+template <class T>
+__global__ void k_halo_unpack(int n, const int* __restrict__ dst, int NA, const T* __restrict__ buf, T* b0, T* b1) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n) return;
+	const T* i = buf + 5 * (size_t)t;
+	const Q5<T> q{i[0], i[1], i[2], i[3], i[4]};
+	st5(b0, NA, dst[t], q);
+	if (b1) st5(b1, NA, dst[t], q);
+}
+
 // ===================================================================== fused
 // Slot data of one real cell.  NSL = 4 is the all-tetrahedron fast path:
 // slots of cell c are 4c..4c+3, so per-slot arrays load as vectors.  NSL = 0

@@ -26,6 +26,12 @@ void launch_smooth(const GeoView&, const StateView&, double* j1, int r0, int r1,
 // ---- shared by both paths, per precision ----
 template <class T>
 void launch_halo(int n, const int* dst, const int* src, int NA, T* b0, T* b1, cudaStream_t);
+// halo entries of a block-sharded case: gather into / scatter from an
+// entry-major buffer of 5 values per entry (k_halo_pack, k_halo_unpack)
+template <class T>
+void launch_halo_pack(int n, const int* src, int NA, const T* P, T* buf, cudaStream_t);
+template <class T>
+void launch_halo_unpack(int n, const int* dst, int NA, const T* buf, T* b0, T* b1, cudaStream_t);
 
 // Per-block reductions written into hist[iter*stride + b*10 + (0..4 norms, 5..9 forces)],
 // iter read from *d_iter (the device iteration counter).

@@ -11,6 +11,16 @@ void launch_halo(int n, const int* dst, const int* src, int NA, T* b0, T* b1, cu
 }
 
 template <class T>
+void launch_halo_pack(int n, const int* src, int NA, const T* P, T* buf, cudaStream_t st) {
+	if (n > 0) k_halo_pack<T><<<(n + 127) / 128, 128, 0, st>>>(n, src, NA, P, buf);
+}
+
+template <class T>
+void launch_halo_unpack(int n, const int* dst, int NA, const T* buf, T* b0, T* b1, cudaStream_t st) {
+	if (n > 0) k_halo_unpack<T><<<(n + 127) / 128, 128, 0, st>>>(n, dst, NA, buf, b0, b1);
+}
+
+template <class T>
 void launch_reduce(const ReduceArgs& a, const T* Rc, const T* Rd, const T* P, cudaStream_t st) {
 	constexpr int THREADS = 256;
 	dim3 grid(a.max_chunks, a.nblocks);

@@ -208,6 +208,59 @@ int e3d_case_history_length(const e3d_solver* s, int case_index, int* n);
 int e3d_case_history(const e3d_solver* s, int case_index, int first, int count, e3d_iter_record* out);
 int e3d_batch_tuning(const e3d_solver* s, int* tile_cells, int* grid, double* ms_per_iter, int* from_cache);
 
+/* ---- block sharding: one case over several processes, one GPU each ------------
+ * Replaces the reference's MPI distribution and transport
+ * (BlockCommunicator::BlockCommunicator, MPI/src/BlockCommunicator.cpp:29-38;
+ * updateBoundaries, :66-211; getMyBlocks, :284-294).  Rank r of n_ranks holds
+ * the case blocks [first_block[r], first_block[r+1]) (first_block has
+ * n_ranks + 1 entries, starts at 0, ends at the block count and rises
+ * strictly).  e3d_shard_first_blocks fills it the reference's way: n_blocks /
+ * n_ranks blocks per rank, one more for the first n_blocks % n_ranks ranks.
+ *
+ * Connexions inside a rank's range stay device copies.  The others are halo
+ * entries of 5 primitives (rho u v w p) that cross ranks, ordered by peer
+ * rank, then by connexion in topology order, then by cell pair: a rank's send
+ * entries for peer r are exactly r's receive entries from it, the layout of
+ * an all-to-all with per-peer counts.  e3d_case_shard_plan lists them on the
+ * host (no GPU): per-peer entry counts, and when cells are non-null the
+ * (block, block-local cell) pair of each entry, [2 * total] int32 each
+ * (origins for send, destination ghosts for recv).
+ *
+ * A shard solver (e3d_shard_create) is an e3d_solver over its blocks; its
+ * block indices are local (block b is case block first_block[rank] + b).  It
+ * advances one iteration per e3d_iterate / e3d_iterate_timed call, and only
+ * after its halo has crossed: before the first iteration and after each one,
+ * e3d_shard_pack gathers the entries the peers need into a device buffer
+ * (sum of send counts x 5 values in the solver's precision: double for
+ * E3D_FP64, float for E3D_FP32), the caller moves the buffers (an all-to-all;
+ * NCCL over NVLink, or host-staged), and e3d_shard_unpack writes the received
+ * entries (device buffer, sum of recv counts x 5) into the ghost cells.  Both
+ * queue work on the solver stream and return without waiting.  Iterating
+ * earlier fails with E3D_ERR_STATE; more than one iteration per call with
+ * E3D_ERR_ARG.
+ *
+ * Norms and forces: e3d_shard_flow_data hands out the raw per-block sums of
+ * the iterations run since its last call ([n][local blocks][10]: five squared
+ * residual sums, then the wall force terms, as e3d_flow_data; *n_iters = n;
+ * `capacity` doubles room, else E3D_ERR_ARG and nothing is taken; out = NULL
+ * only sets *n_iters), and fails with E3D_ERR_NONFINITE when one of them is
+ * not finite.  The caller gathers every rank's, in block order
+ * ([n][all blocks][10]), and hands them to e3d_shard_push_flow_data, which
+ * appends whole-case records to the shard's history, summed in block order
+ * as a single GPU sums them (the reference's MPI build sums per-rank partials
+ * with MPI_Allreduce instead, BlockCommunicator.cpp:299-339).  e3d_solve and
+ * e3d_batch_solve fail on a shard: its stop test needs every rank's norms. */
+int e3d_shard_first_blocks(int n_blocks, int n_ranks, int32_t* first_block);
+int e3d_case_shard_plan(const e3d_case* c, const int32_t* first_block, int n_ranks, int rank, int64_t* send_counts,
+                        int64_t* recv_counts, int32_t* send_cells, int32_t* recv_cells);
+int e3d_shard_create(const e3d_case* c, const int32_t* first_block, int n_ranks, int rank, const e3d_options* opt,
+                     e3d_solver** out);
+int e3d_shard_halo_counts(const e3d_solver* s, int64_t* send_counts, int64_t* recv_counts);
+int e3d_shard_pack(e3d_solver* s, void* send);
+int e3d_shard_unpack(e3d_solver* s, const void* recv);
+int e3d_shard_flow_data(e3d_solver* s, double* out, int64_t capacity, int* n_iters);
+int e3d_shard_push_flow_data(e3d_solver* s, const double* all_blocks, int n_iters);
+
 /* ---- precision switch, warm start and the learned surrogate -------------------
  * No counterpart in the reference.
  * e3d_solver_set_precision: an FP32 solver becomes an FP64 solver in place
