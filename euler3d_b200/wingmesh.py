@@ -180,10 +180,29 @@ def wing_mesh(w: WingSpec, n_points: int, seed: int = 5):
     return pts, tets
 
 
-def split_blocks(w: WingSpec, pts: np.ndarray, tets: np.ndarray, n_blocks: int) -> list[mg.BlockMesh]:
-    """x-slab blocks of equal cell count, Morton-ordered cells, markers
-    WALL, FARFIELD, SYMMETRY, then one CONNEXION per neighbouring block."""
+def _box_kinds(w: WingSpec, pts: np.ndarray):
+    """Boundary faces of the Delaunay box: SYMMETRY on z = 0, FARFIELD on the
+    other box faces, WALL for the rest (the faces the removed tets exposed)."""
     x0, x1, y0, y1, z0, z1 = w.box
+
+    def kinds(fnodes: np.ndarray):
+        fx = pts[fnodes]  # (faces, 3 nodes, 3)
+        on = {}
+        for name, axis, val in (("x0", 0, x0), ("x1", 0, x1), ("y0", 1, y0), ("y1", 1, y1), ("z0", 2, z0),
+                                ("z1", 2, z1)):
+            on[name] = np.all(fx[:, :, axis] == val, axis=1)
+        sym = on["z0"]
+        far = ~sym & (on["x0"] | on["x1"] | on["y0"] | on["y1"] | on["z1"])
+        return sym, far
+    return kinds
+
+
+def split_blocks(w: WingSpec, pts: np.ndarray, tets: np.ndarray, n_blocks: int, kinds=None) -> list[mg.BlockMesh]:
+    """x-slab blocks of equal cell count, Morton-ordered cells, markers
+    WALL, FARFIELD, SYMMETRY, then one CONNEXION per neighbouring block.
+    ``kinds(face_nodes) -> (symmetry, farfield)`` labels the boundary faces
+    (the rest are WALL); by default the faces of the Delaunay box."""
+    kinds = kinds or _box_kinds(w, pts)
     cen = pts[tets].mean(axis=1)
     order = np.argsort(cen[:, 0], kind="stable")
     blk_of = np.empty(tets.shape[0], dtype=np.int64)
@@ -211,15 +230,11 @@ def split_blocks(w: WingSpec, pts: np.ndarray, tets: np.ndarray, n_blocks: int) 
     mate[srt[pair_first + 1]] = srt[pair_first]
     bnd = mate < 0
     bidx = np.nonzero(bnd)[0]
-    fx = pts[faces[bidx]]  # (boundary faces, 3 nodes, 3)
-    on = {}
-    for name, axis, val in (("x0", 0, x0), ("x1", 0, x1), ("y0", 1, y0), ("y1", 1, y1), ("z0", 2, z0), ("z1", 2, z1)):
-        on[name] = np.all(fx[:, :, axis] == val, axis=1)
     sym = np.zeros(faces.shape[0], bool)
     far = np.zeros(faces.shape[0], bool)
     wall = np.zeros(faces.shape[0], bool)
-    sym[bidx] = on["z0"]
-    far[bidx] = ~on["z0"] & (on["x0"] | on["x1"] | on["y0"] | on["y1"] | on["z1"])
+    sym[bidx], far[bidx] = kinds(faces[bidx])
+    far[bidx] &= ~sym[bidx]
     wall[bidx] = ~sym[bidx] & ~far[bidx]
     fblock = blk_of[owner]
     mblock = np.where(mate >= 0, blk_of[owner[np.maximum(mate, 0)]], -1)
@@ -270,4 +285,168 @@ def write_wing_case(directory: str, n_points: int, n_blocks: int = 16, seed: int
     os.makedirs(os.path.join(directory, "bin"), exist_ok=True)
     counts = {t: int(sum(f.shape[0] for blk in blocks for tg, f in blk.markers if tg == t))
               for t in ("WALL", "FARFIELD", "SYMMETRY", "CONNEXION")}
+    return path, {"points": int(pts.shape[0]), "tets": int(tets.shape[0]), "blocks": n_blocks, **counts}
+
+
+# ---------------------------------------------------------------- body-fitted
+# The same wing meshed with a boundary-conforming structured grid: in every
+# spanwise station an O-grid around the section (node i at angle
+# theta = 2 pi (i + 1/2) / ni from the trailing edge, upper surface for
+# i < ni / 2), j = 0 on the wall, j = nj on a wind-tunnel rectangle reached
+# along rays from the section's mid-chord; stations k cluster toward the tip.
+# The half-step offset puts no node exactly at the leading or trailing edge,
+# so no cell has three corners on one line.  The section thickness falls to
+# zero over a rounded tip; from the tip station outward the section is a
+# slit: the lower node i and the upper node ni - 1 - i of the j = 0 ring are
+# one node, so the cells above and below share faces, and the two cells
+# around the slit's leading and trailing edges become prisms.  Each
+# hexahedron splits into the 6 Kuhn tetrahedra around its (0,0,0)-(1,1,1)
+# diagonal, in i-mirrored local coordinates for the lower half (i >= ni / 2):
+# every shared face, the slit's included, then gets the same diagonal from both
+# sides, so the tetrahedra are conforming; the tetrahedra of a collapsed edge
+# (two corners one node) have no volume and are left out.
+@dataclass
+class TunnelSpec:
+    x0: float = -6.0   # inlet plane (FARFIELD)
+    x1: float = 8.0    # outlet plane (FARFIELD)
+    h: float = 6.0     # y = -h and y = +h planes (SYMMETRY)
+    z1: float = 4.0    # far spanwise plane (SYMMETRY); z = 0 is the root's SYMMETRY plane
+    wall_spacing: float = 0.004  # first cell height off the wall (root chords)
+    tip_round: float = 0.06      # span over which the thickness falls to zero (elliptic cap)
+
+
+def _stretch(n: int, first: float, length: float) -> np.ndarray:
+    """n + 1 monotone offsets 0..length, the first step `first`, geometric growth."""
+    if first * n >= length:
+        return np.linspace(0.0, length, n + 1)
+    lo, hi = 1.0 + 1e-12, 2.0
+    while first * (hi ** n - 1) / (hi - 1) < length:
+        hi *= 2.0
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if first * (r ** n - 1) / (r - 1) < length:
+            lo = r
+        else:
+            hi = r
+    r = 0.5 * (lo + hi)
+    d = first * r ** np.arange(n)
+    x = np.concatenate([[0.0], np.cumsum(d)])
+    return x * (length / x[-1])
+
+
+def _stations(w: WingSpec, t: TunnelSpec, nk_wing: int, nk_out: int) -> np.ndarray:
+    b = w.semi_span
+    zw = b * np.sin(0.5 * np.pi * np.arange(nk_wing + 1) / nk_wing)
+    zw[-1] = b
+    zo = b + _stretch(nk_out, zw[-1] - zw[-2], t.z1 - b)
+    return np.concatenate([zw, zo[1:]])
+
+
+def _thickness_factor(w: WingSpec, t: TunnelSpec, z: np.ndarray) -> np.ndarray:
+    zr = w.semi_span - t.tip_round
+    u = np.clip((z - zr) / t.tip_round, 0.0, 1.0)
+    return np.where(z >= w.semi_span, 0.0, np.sqrt(np.maximum(0.0, 1.0 - u * u)))
+
+
+def _ray_to_box(cx: float, theta: np.ndarray, t: TunnelSpec) -> np.ndarray:
+    """Where rays from (cx, 0) at angle theta meet the rectangle [x0,x1] x [-h,h]."""
+    c, s = np.cos(theta), np.sin(theta)
+    with np.errstate(divide="ignore"):
+        tx = np.where(c > 0, (t.x1 - cx) / c, np.where(c < 0, (t.x0 - cx) / c, np.inf))
+        ty = np.where(s != 0, t.h / np.abs(s), np.inf)
+    r = np.minimum(tx, ty)
+    x, y = cx + r * c, r * s
+    x = np.where(tx <= ty, np.where(c > 0, t.x1, t.x0), x)  # exactly on the planes
+    y = np.where(ty <= tx, np.sign(s) * t.h, y)
+    return np.stack([x, y], axis=1)
+
+
+_MIRROR = np.array([b ^ 1 for b in range(8)])  # corner (a, b, c) -> (1 - a, b, c)
+
+
+def body_fitted_wing(w: WingSpec, ni: int, nj: int, nk_wing: int, nk_out: int, t: TunnelSpec | None = None):
+    """Nodes, tetrahedra and boundary-face labeller of the body-fitted mesh."""
+    t = t or TunnelSpec()
+    if ni % 2:
+        raise ValueError("ni must be even (the leading edge is node ni / 2)")
+    z = _stations(w, t, nk_wing, nk_out)
+    nk = z.size - 1
+    theta = 2.0 * np.pi * (np.arange(ni) + 0.5) / ni
+    s_c = 0.5 * (1.0 + np.cos(theta))  # chord fraction: near 1 at the trailing edge, near 0 at the leading edge
+    upper = np.arange(ni) < ni // 2
+    g = _stretch(nj, t.wall_spacing / 6.0, 1.0)  # ray fraction; first step ~ wall_spacing on a 6-chord ray
+    X = np.empty((ni, nj + 1, nk + 1, 3))
+    for k in range(nk + 1):
+        xle, c = _le_chord(w, np.array([min(z[k], w.semi_span)]))
+        xle, c = float(xle[0]), float(c[0])
+        yt = c * naca_half_thickness(s_c, w.thickness) * _thickness_factor(w, t, np.array([z[k]]))[0]
+        inner = np.stack([xle + s_c * c, np.where(upper, yt, -yt)], axis=1)
+        outer = _ray_to_box(xle + 0.5 * c, theta, t)
+        X[:, :, k, 0:2] = inner[:, None, :] + g[None, :, None] * (outer - inner)[:, None, :]
+        X[:, :, k, 2] = z[k]
+    # node ids with the slit identified: from the tip station outward, the
+    # lower-surface node i of ring j = 0 is the upper node ni - 1 - i
+    kt = nk_wing
+    nid = np.arange(ni * (nj + 1) * (nk + 1)).reshape(ni, nj + 1, nk + 1)
+    low = np.arange(ni // 2, ni)
+    ks = np.arange(kt, nk + 1)[None, :]
+    nid[low[:, None], 0, ks] = nid[(ni - 1 - low)[:, None], 0, ks]
+    used, inv = np.unique(nid.ravel(), return_inverse=True)
+    pts = X.reshape(-1, 3)[used]
+    nid = inv.reshape(nid.shape)
+    # hexahedra (i, j, k) -> 8 corners, bit 0: i + 1, bit 1: j + 1, bit 2: k + 1
+    hi, hj, hk = np.meshgrid(np.arange(ni), np.arange(nj), np.arange(nk), indexing="ij")
+    hi, hj, hk = hi.ravel(), hj.ravel(), hk.ravel()
+    corners = np.stack([nid[(hi + (b & 1)) % ni, hj + ((b >> 1) & 1), hk + ((b >> 2) & 1)] for b in range(8)], axis=1)
+    lower = hi >= ni // 2
+    corners[lower] = corners[lower][:, _MIRROR]
+    tets = corners[:, mg._KUHN_TETS].reshape(-1, 4)
+    st = np.sort(tets, axis=1)
+    tets = tets[np.all(st[:, 1:] != st[:, :-1], axis=1)]  # collapsed edges: no volume
+
+    # node flags for the boundary labels: 1 on the inlet or outlet plane,
+    # 4 on z = 0, 8 on the far spanwise plane, 16 on the outer ring
+    ring = np.zeros(nid.shape, np.int8)
+    ox = X[:, nj, :, 0]
+    ring[:, nj, :] |= np.where((ox == t.x0) | (ox == t.x1), 17, 16).astype(np.int8)
+    ring[:, :, 0] |= 4
+    ring[:, :, nk] |= 8
+    flag = np.zeros(pts.shape[0], np.int8)
+    np.bitwise_or.at(flag, nid.ravel(), ring.ravel())
+
+    def kinds(fnodes: np.ndarray):
+        """SYMMETRY: the z = 0 and far spanwise planes and the tunnel's y = -h
+        and y = +h sides; FARFIELD: the inlet and outlet planes, and the ring
+        faces that cut a corner of the tunnel between one of them and a side."""
+        f = flag[fnodes]
+        zsym = np.all((f & 4) != 0, axis=1) | np.all((f & 8) != 0, axis=1)
+        on_ring = np.all((f & 16) != 0, axis=1) & ~zsym
+        inout = np.any((f & 1) != 0, axis=1)
+        return zsym | (on_ring & ~inout), on_ring & inout
+
+    return pts, tets, kinds
+
+
+def write_body_fitted_wing_case(directory: str, ni: int, nj: int, nk_wing: int, nk_out: int, n_blocks: int = 16,
+                                prefix: str = "wing", deck: mg.Deck | None = None, spec: WingSpec | None = None,
+                                tunnel: TunnelSpec | None = None) -> tuple[str, dict]:
+    """Generate, split and write the body-fitted wing case; returns (deck path, summary)."""
+    w = spec or WingSpec()
+    os.makedirs(directory, exist_ok=True)
+    pts, tets, kinds = body_fitted_wing(w, ni, nj, nk_wing, nk_out, tunnel)
+    blocks = split_blocks(w, pts, tets, n_blocks, kinds)
+    files = []
+    for b, blk in enumerate(blocks):
+        name = f"{prefix}_B{b}.su2"
+        mg.write_su2(os.path.join(directory, name), blk)
+        files.append(name)
+    top = f"{prefix}.top"
+    mg.write_topology(os.path.join(directory, top), files, blocks)
+    d = deck or mg.Deck(topology=top)
+    d.topology = top
+    path = os.path.join(directory, f"{prefix}.deck")
+    mg.write_deck(path, d)
+    os.makedirs(os.path.join(directory, "bin"), exist_ok=True)
+    counts = {tg: int(sum(f.shape[0] for blk in blocks for t_, f in blk.markers if t_ == tg))
+              for tg in ("WALL", "FARFIELD", "SYMMETRY", "CONNEXION")}
     return path, {"points": int(pts.shape[0]), "tets": int(tets.shape[0]), "blocks": n_blocks, **counts}

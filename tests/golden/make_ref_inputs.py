@@ -31,6 +31,10 @@ files by this script; nothing at test time reads the reference checkout):
   and the unmodified reference program ends with a segmentation fault while
   building block 0's faces (the host library rejects the file with
   E3D_ERR_FORMAT).
+* wing_body_fitted_16x4x8: not a reference file: the body-fitted swept wing
+  of the large configuration (euler3d_b200.wingmesh) at a small size, packed
+  the same way so that its fixture does not depend on the generator staying
+  unchanged.
 
 For every case in CASES the compiled reference driver (oracle/_ref/
 e3d_refdriver, the reference's own solver objects) runs the deck; the fixture
@@ -90,6 +94,12 @@ CASES = {
                                      deck=dict(order=2, flux="roe", gradient="leastsquares",
                                                limiter="venkatakrishnan", k=5.0, omega=OMEGA, mach=0.8,
                                                aoa_deg=1.25, cfl=1.5)),
+    # the swept-wing configuration's scheme (AUSM + LS + Venkatakrishnan, M 0.8, alpha 3) on the
+    # body-fitted wing mesh
+    "ref_wingbf_o2_ls_venk_ausm": dict(input="wing_body_fitted_16x4x8", iters=20,
+                                       deck=dict(order=2, flux="ausm", gradient="leastsquares",
+                                                 limiter="venkatakrishnan", k=5.0, omega=OMEGA, mach=0.8,
+                                                 aoa_deg=3.0, cfl=1.5)),
 }
 
 STAGE_KEYS = ("w0", "dt", "spectral_radius", "grad", "limiter", "conv_res", "diss_res")
@@ -201,8 +211,21 @@ def onera_files() -> dict[str, bytes]:
     return files
 
 
+def wing_files() -> dict[str, bytes]:
+    """The body-fitted swept wing of the large configuration at a small size
+    (euler3d_b200.wingmesh: O-grid sections, rounded tip, slit beyond it,
+    tunnel box), 16 x 4 x (6 + 2) hexahedra split into tetrahedra, 2 blocks."""
+    from euler3d_b200 import wingmesh as wm
+
+    with tempfile.TemporaryDirectory() as td:
+        wm.write_body_fitted_wing_case(td, 16, 4, 6, 2, n_blocks=2, prefix="wing")
+        return {f: open(os.path.join(td, f), "rb").read() for f in sorted(os.listdir(td))
+                if f.endswith((".su2", ".top"))}
+
+
 INPUTS = {"naca0012_coarse": (naca_files, "naca0012_coarse.top"),
-          "onera_m6_160b_sub12": (onera_files, "onera_sub.top")}
+          "onera_m6_160b_sub12": (onera_files, "onera_sub.top"),
+          "wing_body_fitted_16x4x8": (wing_files, "wing.top")}
 
 
 def pack(files: dict[str, bytes]) -> bytes:

@@ -56,3 +56,42 @@ def test_wing_geometry():
     z = 0.75
     assert wm.inside_wing(w, np.array([[z * np.tan(np.radians(30)) + 0.05, 0.0, z]]))[0]
     assert not wm.inside_wing(w, np.array([[z * np.tan(np.radians(30)) - 0.01, 0.0, z]]))[0]
+
+
+@pytest.mark.parametrize("ni,nj,nkw,nko", [(16, 4, 6, 2), (32, 8, 12, 4)])
+def test_body_fitted_wing_is_conforming(ni, nj, nkw, nko):
+    """The structured wing: every triangle is shared by at most two tets (the
+    slit beyond the tip included), no tet is flat, the wall is exactly the
+    wing surface (2 triangles per surface quad, one fewer at each of the two
+    collapsed tip edges), and the domain is the tunnel minus the wing."""
+    w, t = wm.WingSpec(), wm.TunnelSpec()
+    pts, tets, kinds = wm.body_fitted_wing(w, ni, nj, nkw, nko)
+    p = pts[tets]
+    vol = np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), p[:, 3] - p[:, 0]) / 6
+    assert np.all(np.abs(vol) > 0)
+    faces = np.sort(tets[:, [[0, 1, 2], [0, 1, 3], [0, 2, 3], [1, 2, 3]]].reshape(-1, 3), axis=1)
+    u, c = np.unique(faces, axis=0, return_counts=True)
+    assert set(np.unique(c)) == {1, 2}
+    bnd = u[c == 1]
+    sym, far = kinds(bnd)
+    wall = ~sym & ~far
+    assert wall.sum() == 2 * ni * nkw - 2
+    wp = pts[bnd[wall]]
+    assert wp[:, :, 2].max() <= w.semi_span and np.all(wm.inside_wing(w, wp.mean(axis=1) * [1, 0, 1]))
+    fp = pts[bnd[far]]
+    assert np.all(np.isin(fp[:, :, 0], [t.x0, t.x1]).any(axis=1))  # inlet, outlet and their corner cuts
+    box = (t.x1 - t.x0) * 2 * t.h * t.z1  # less the wing and the tunnel corners the outer ring cuts off
+    assert box * 0.9 < np.abs(vol).sum() < box
+
+
+def test_body_fitted_wing_case_loads(tmp_path):
+    deck = mg.Deck(topology="", order=2, flux="ausm", gradient="leastsquares", limiter="venkatakrishnan", mach=0.8,
+                   aoa_deg=3.0)
+    path, summ = wm.write_body_fitted_wing_case(str(tmp_path), 24, 6, 8, 3, n_blocks=3, deck=deck)
+    case = api.Case(path)  # closed cells, every boundary face on a marker
+    n = [case.block_info(b).n_real for b in range(3)]
+    assert sum(n) == summ["tets"] and max(n) - min(n) <= 1
+    for b in range(3):
+        assert np.all(np.isfinite(case.get(b, "ls_weights")))
+        assert np.all(case.get(b, "cell_volume")[:n[b]] > 0)
+    assert sum(case.block_info(b).n_wall_faces for b in range(3)) == summ["WALL"] == 2 * 24 * 8 - 2
