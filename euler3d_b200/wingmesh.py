@@ -43,10 +43,13 @@ class WingSpec:
     box: tuple = (-4.0, 6.0, -5.0, 5.0, 0.0, 4.0)
 
 
-def naca_half_thickness(s: np.ndarray, t: float) -> np.ndarray:
-    """NACA 4-digit thickness distribution (closed trailing edge), chord 1."""
+def naca_half_thickness(s: np.ndarray, t: float, closed: bool = True) -> np.ndarray:
+    """NACA 4-digit thickness distribution, chord 1: the closed trailing-edge
+    variant (last coefficient 0.1036) or the published one (0.1015, a blunt
+    trailing edge 0.021 t thick)."""
     s = np.clip(s, 0.0, 1.0)
-    return 5.0 * t * (0.2969 * np.sqrt(s) - 0.1260 * s - 0.3516 * s ** 2 + 0.2843 * s ** 3 - 0.1036 * s ** 4)
+    a4 = 0.1036 if closed else 0.1015
+    return 5.0 * t * (0.2969 * np.sqrt(s) - 0.1260 * s - 0.3516 * s ** 2 + 0.2843 * s ** 3 - a4 * s ** 4)
 
 
 def _le_chord(w: WingSpec, z):
@@ -289,30 +292,35 @@ def write_wing_case(directory: str, n_points: int, n_blocks: int = 16, seed: int
 
 
 # ---------------------------------------------------------------- body-fitted
-# The same wing meshed with a boundary-conforming structured grid: in every
-# spanwise station an O-grid around the section (node i at angle
-# theta = 2 pi (i + 1/2) / ni from the trailing edge, upper surface for
-# i < ni / 2), j = 0 on the wall, j = nj on a wind-tunnel rectangle reached
-# along rays from the section's mid-chord; stations k cluster toward the tip.
-# The half-step offset puts no node exactly at the leading or trailing edge,
-# so no cell has three corners on one line.  The section thickness falls to
-# zero over a rounded tip; from the tip station outward the section is a
-# slit: the lower node i and the upper node ni - 1 - i of the j = 0 ring are
-# one node, so the cells above and below share faces, and the two cells
-# around the slit's leading and trailing edges become prisms.  Each
-# hexahedron splits into the 6 Kuhn tetrahedra around its (0,0,0)-(1,1,1)
-# diagonal, in i-mirrored local coordinates for the lower half (i >= ni / 2):
-# every shared face, the slit's included, then gets the same diagonal from both
-# sides, so the tetrahedra are conforming; the tetrahedra of a collapsed edge
-# (two corners one node) have no volume and are left out.
+# The same wing meshed with a boundary-conforming structured grid.  In every
+# spanwise station an O-grid wraps the section: node i sits at angle
+# theta = 2 pi (i + 1/2) / ni from the trailing edge (upper surface for
+# i < ni / 2) at chord fraction s = 1 - sin(theta / 2), clustered at the
+# leading edge; the section is the published NACA thickness polynomial with
+# its blunt trailing edge, whose base is the face between nodes ni - 1 and 0.
+# Ring j = 0 is the wall, ring j = nj a wind-tunnel rectangle reached along
+# rays from the section's mid-chord, with geometric growth from a first layer
+# about as thick as the steps around the section.  Stations k cluster toward
+# the tip, where the thickness falls to zero over a rounded cap; from the tip
+# station outward the section is a slit: the lower node i and the upper node
+# ni - 1 - i of ring j = 0 are one node, so the cells above and below share
+# faces, and the two cells around the slit's leading and trailing edges
+# become prisms.  With tip_round = 0 and no stations beyond the tip, the wing
+# spans the tunnel instead (its tip section on the far SYMMETRY plane).
+# Each hexahedron splits into the 6 Kuhn tetrahedra around its
+# (0,0,0)-(1,1,1) diagonal, in i-mirrored local coordinates for the lower half
+# (i >= ni / 2): every shared face, the slit's included, then gets the same
+# diagonal from both sides, so the tetrahedra are conforming; the tetrahedra
+# of a collapsed edge (two corners one node) have no volume and are left out.
 @dataclass
 class TunnelSpec:
     x0: float = -6.0   # inlet plane (FARFIELD)
     x1: float = 8.0    # outlet plane (FARFIELD)
     h: float = 6.0     # y = -h and y = +h planes (SYMMETRY)
     z1: float = 4.0    # far spanwise plane (SYMMETRY); z = 0 is the root's SYMMETRY plane
-    wall_spacing: float = 0.004  # first cell height off the wall (root chords)
-    tip_round: float = 0.06      # span over which the thickness falls to zero (elliptic cap)
+    wall_spacing: float | None = None  # first cell height off the wall (root chords); None: 2 / ni, about the
+    #                                    mean step around the section, so the cells at the wall are near cubes
+    tip_round: float = 0.06      # span over which the thickness falls to zero (elliptic cap); 0: no tip
 
 
 def _stretch(n: int, first: float, length: float) -> np.ndarray:
@@ -336,6 +344,8 @@ def _stretch(n: int, first: float, length: float) -> np.ndarray:
 
 def _stations(w: WingSpec, t: TunnelSpec, nk_wing: int, nk_out: int) -> np.ndarray:
     b = w.semi_span
+    if nk_out == 0:  # the wing spans the tunnel (its far plane at the tip section)
+        return np.linspace(0.0, b, nk_wing + 1)
     zw = b * np.sin(0.5 * np.pi * np.arange(nk_wing + 1) / nk_wing)
     zw[-1] = b
     zo = b + _stretch(nk_out, zw[-1] - zw[-2], t.z1 - b)
@@ -343,6 +353,8 @@ def _stations(w: WingSpec, t: TunnelSpec, nk_wing: int, nk_out: int) -> np.ndarr
 
 
 def _thickness_factor(w: WingSpec, t: TunnelSpec, z: np.ndarray) -> np.ndarray:
+    if t.tip_round <= 0.0:  # the wing spans the tunnel: no tip
+        return np.ones_like(z)
     zr = w.semi_span - t.tip_round
     u = np.clip((z - zr) / t.tip_round, 0.0, 1.0)
     return np.where(z >= w.semi_span, 0.0, np.sqrt(np.maximum(0.0, 1.0 - u * u)))
@@ -372,14 +384,18 @@ def body_fitted_wing(w: WingSpec, ni: int, nj: int, nk_wing: int, nk_out: int, t
     z = _stations(w, t, nk_wing, nk_out)
     nk = z.size - 1
     theta = 2.0 * np.pi * (np.arange(ni) + 0.5) / ni
-    s_c = 0.5 * (1.0 + np.cos(theta))  # chord fraction: near 1 at the trailing edge, near 0 at the leading edge
+    # chord fraction: clustered at the leading edge (s ~ (pi - theta)^2), even
+    # steps at the blunt trailing edge (whose base is the face from node ni - 1
+    # to node 0)
+    s_c = 1.0 - np.sin(0.5 * theta)
     upper = np.arange(ni) < ni // 2
-    g = _stretch(nj, t.wall_spacing / 6.0, 1.0)  # ray fraction; first step ~ wall_spacing on a 6-chord ray
+    first = t.wall_spacing if t.wall_spacing is not None else 2.0 * w.root_chord / ni
+    g = _stretch(nj, first / 6.0, 1.0)  # ray fraction; first step ~ `first` on a 6-chord ray
     X = np.empty((ni, nj + 1, nk + 1, 3))
     for k in range(nk + 1):
         xle, c = _le_chord(w, np.array([min(z[k], w.semi_span)]))
         xle, c = float(xle[0]), float(c[0])
-        yt = c * naca_half_thickness(s_c, w.thickness) * _thickness_factor(w, t, np.array([z[k]]))[0]
+        yt = c * naca_half_thickness(s_c, w.thickness, closed=False) * _thickness_factor(w, t, np.array([z[k]]))[0]
         inner = np.stack([xle + s_c * c, np.where(upper, yt, -yt)], axis=1)
         outer = _ray_to_box(xle + 0.5 * c, theta, t)
         X[:, :, k, 0:2] = inner[:, None, :] + g[None, :, None] * (outer - inner)[:, None, :]
@@ -388,9 +404,10 @@ def body_fitted_wing(w: WingSpec, ni: int, nj: int, nk_wing: int, nk_out: int, t
     # lower-surface node i of ring j = 0 is the upper node ni - 1 - i
     kt = nk_wing
     nid = np.arange(ni * (nj + 1) * (nk + 1)).reshape(ni, nj + 1, nk + 1)
-    low = np.arange(ni // 2, ni)
-    ks = np.arange(kt, nk + 1)[None, :]
-    nid[low[:, None], 0, ks] = nid[(ni - 1 - low)[:, None], 0, ks]
+    if nk_out > 0:
+        low = np.arange(ni // 2, ni)
+        ks = np.arange(kt, nk + 1)[None, :]
+        nid[low[:, None], 0, ks] = nid[(ni - 1 - low)[:, None], 0, ks]
     used, inv = np.unique(nid.ravel(), return_inverse=True)
     pts = X.reshape(-1, 3)[used]
     nid = inv.reshape(nid.shape)
