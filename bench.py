@@ -60,8 +60,14 @@ def make_case(directory: str, n: int, blocks: int) -> str:
     return mg.write_case(directory, n, blocks, deck=deck)
 
 
-WING_SCHEME = dict(order=2, flux="ausm", gradient="leastsquares", limiter="barthjespersen", omega=2.16e-16, k=5.0,
+# the swept-wing configuration: AUSM + least squares + Venkatakrishnan (K = 5), M 0.8, alpha 3
+WING_SCHEME = dict(order=2, flux="ausm", gradient="leastsquares", limiter="venkatakrishnan", omega=2.16e-16, k=5.0,
                    mach=0.8, aoa_deg=3.0, cfl=1.5, stages=5)
+# body-fitted mesh: O-grid points around each section x layers off the wall x spanwise stations
+# (wing, beyond the tip): 256 x 80 x (112 + 48) hexahedra, 6 tetrahedra each
+WING_DIMS = (256, 80, 112, 48)
+# the earlier Delaunay mesh (--wing-mesh delaunay): seeded points, staircase wall
+WING_DELAUNAY_SCHEME = dict(WING_SCHEME, limiter="barthjespersen")
 WING_POINTS = 3_800_000
 
 
@@ -70,17 +76,28 @@ def wing_case(a, td):
     from euler3d_b200 import meshgen as mg
     from euler3d_b200 import wingmesh as wm
 
+    delaunay = a.wing_mesh == "delaunay"
+    w = WING_DELAUNAY_SCHEME if delaunay else WING_SCHEME
     if a.mesh_dir and os.path.exists(os.path.join(a.mesh_dir, "wing.deck")):
         case_dir = a.mesh_dir
     else:
         case_dir = a.mesh_dir or os.path.join(td, "wing")
-        deck = mg.Deck(topology="", max_iter=1000000, criterion=-15.0, **WING_SCHEME)
-        wm.write_wing_case(case_dir, WING_POINTS, n_blocks=16, seed=5, deck=deck)
-    w = WING_SCHEME
-    cfg = {"workload": f"swept trapezoidal wing (NACA 4-digit 12 %, 30 deg sweep, taper 0.56) in a farfield box, "
-                       f"seeded Delaunay tetrahedra (seed 5, {WING_POINTS:,} points requested), 16 x-slab blocks on "
-                       f"one GPU, Morton-ordered cells; {w['gradient']} + {w['limiter']} + {w['flux']}, "
-                       f"M {w['mach']}, alpha {w['aoa_deg']}, {w['stages']}-stage RK, CFL {w['cfl']}",
+        deck = mg.Deck(topology="", max_iter=1000000, criterion=-15.0, **w)
+        if delaunay:
+            wm.write_wing_case(case_dir, WING_POINTS, n_blocks=16, seed=5, deck=deck)
+        else:
+            wm.write_body_fitted_wing_case(case_dir, *WING_DIMS, n_blocks=16, deck=deck)
+    scheme = (f"{w['gradient']} + {w['limiter']} (K = {w['k']:g}) + {w['flux']}, M {w['mach']}, alpha "
+              f"{w['aoa_deg']}, {w['stages']}-stage RK, CFL {w['cfl']}")
+    if delaunay:
+        mesh = (f"in a farfield box, seeded Delaunay tetrahedra (seed 5, {WING_POINTS:,} points requested), wall "
+                f"left by the removed interior tetrahedra")
+    else:
+        ni, nj, nkw, nko = WING_DIMS
+        mesh = (f"in a tunnel box (inlet/outlet farfield, sides symmetry), body-fitted: O-grid sections of {ni} x "
+                f"{nj} hexahedra, {nkw} + {nko} spanwise stations, rounded tip, 6 tetrahedra per hexahedron")
+    cfg = {"workload": f"swept trapezoidal wing (NACA 4-digit 12 %, 30 deg sweep, taper 0.56) {mesh}; 16 x-slab "
+                       f"blocks on one GPU, Morton-ordered cells; {scheme}",
            "blocks": 16,
            "arithmetic": "fp32 fluxes/gradients/limiters, fp64 conserved state and reductions"
            if a.precision == "fp32" else "fp64 throughout (reference arithmetic)",
@@ -608,7 +625,10 @@ def main():
     ap.add_argument("--workload", choices=["channel", "polar", "warmstart", "wing"], default="channel",
                     help="channel: the 3.07M-tet second-order case (default); polar: 64-case batched sweep "
                          "throughput; warmstart: time to an 8-order drop, batched + learned vs plain; wing: the "
-                         "~20M-tet Delaunay swept wing")
+                         "~20M-tet swept wing")
+    ap.add_argument("--wing-mesh", choices=["body-fitted", "delaunay"], default="body-fitted",
+                    help="wing: the body-fitted structured mesh (conforming wall; default) or the seeded Delaunay "
+                         "point cloud")
     ap.add_argument("--mesh-dir", default=None,
                     help="wing: a directory holding wing.deck (written by euler3d_b200.wingmesh); generated "
                          "into a temporary directory when absent")

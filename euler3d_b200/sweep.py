@@ -198,6 +198,42 @@ def train_warmstart(out: str, n_cases: int = 200, n_range=(25, 60), steps: int =
     return info
 
 
+# The swept-wing configuration's warm start: the surrogate learns converged
+# states of a coarse body-fitted wing over Mach and alpha and warm-starts the
+# fine mesh.  Its inputs (cell centre, distance to the wall, Mach, alpha) do
+# not depend on the mesh, so a surrogate trained on one resolution applies to
+# another of the same geometry.
+WING_SCHEME = dict(order=2, flux="ausm", gradient="leastsquares", limiter="venkatakrishnan", k=5.0,
+                   omega=2.16e-16, stages=5, cfl=1.5)
+WING_TRAIN_SEED = 3000
+
+
+def wing_points(seed: int, count: int, mach_range=(0.5, 0.85), aoa_range=(0.0, 5.0)) -> list[tuple[float, float]]:
+    """Seeded (Mach, alpha) points, uniform in both (numpy PCG64)."""
+    rng = np.random.default_rng(seed)
+    mach = rng.uniform(mach_range[0], mach_range[1], count)
+    aoa = rng.uniform(aoa_range[0], aoa_range[1], count)
+    return [(round(float(m), 4), round(float(a), 4)) for m, a in zip(mach, aoa)]
+
+
+def write_wing_cases(directory: str, dims: tuple, points: list[tuple[float, float]], scheme: dict = WING_SCHEME,
+                     n_blocks: int = 1) -> list[str]:
+    """One body-fitted wing mesh (dims: ni, nj, nk_wing, nk_out) and one deck
+    per (Mach, alpha) point, all naming the same topology; returns the decks."""
+    from . import wingmesh as wm
+
+    def deck(m, a):
+        return mg.Deck(topology="wing.top", mach=m, aoa_deg=a, max_iter=1000000, criterion=-15.0, **scheme)
+
+    first, _ = wm.write_body_fitted_wing_case(directory, *dims, n_blocks=n_blocks, deck=deck(*points[0]))
+    decks = [first]
+    for i, (m, a) in enumerate(points[1:], 1):
+        path = os.path.join(directory, f"wing_{i}.deck")
+        mg.write_deck(path, deck(m, a))
+        decks.append(path)
+    return decks
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="Train the warm-start surrogate on the seeded channel sweep.")
     ap.add_argument("command", choices=["train"])
