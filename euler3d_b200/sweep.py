@@ -234,14 +234,54 @@ def write_wing_cases(directory: str, dims: tuple, points: list[tuple[float, floa
     return decks
 
 
+# the wing's time to an 8-order drop runs first-order AUSM (the second-order
+# scheme has no 8-order drop on airfoil and wing meshes)
+WING_WARM_SCHEME = dict(order=1, flux="ausm", stages=5, cfl=1.5)
+
+
+def wing_warmstart(n_train: int = 32, train_dims=(64, 20, 24, 8), target_dims=(128, 40, 48, 16), mach: float = 0.8,
+                   aoa: float = 3.0, criterion: float = -8.0, out: str | None = None,
+                   workdir: str | None = None) -> dict:
+    """Trains the surrogate on n_train coarse wings (seeded Mach/alpha, solved
+    to -4 in FP32), then times the target wing from freestream to `criterion`:
+    plain (FP64 drop-in path) against learned (warm start, FP32 to its floor,
+    FP64 with contraction to the criterion)."""
+    import tempfile
+
+    rec = dict(n_train=n_train, train_dims=list(train_dims), target_dims=list(target_dims), mach=mach, aoa=aoa,
+               criterion=criterion, scheme=WING_WARM_SCHEME)
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        pts = wing_points(WING_TRAIN_SEED, n_train)
+        cases = [api.Case(d) for d in write_wing_cases(os.path.join(td, "train"), train_dims, pts,
+                                                        scheme=WING_WARM_SCHEME)]
+        m, info = train_surrogate(cases, seed=WING_TRAIN_SEED, criterion=-4.0, steps=40000, group=16)
+        rec["train"] = info
+        if out:
+            save_surrogate(m, out, dict(info, points=pts, dims=list(train_dims), scheme=WING_WARM_SCHEME))
+        target = api.Case(write_wing_cases(os.path.join(td, "target"), target_dims, [(mach, aoa)],
+                                           scheme=WING_WARM_SCHEME)[0])
+        rec["plain"] = solve_plain(target, criterion, 1000000, check_every=100)
+        rec["learned"] = solve_batched([target], criterion, 1000000, surrogate=m)
+        rec["speedup"] = rec["plain"]["wall_s"] / rec["learned"]["wall_s"]
+        for c in cases + [target]:
+            c.close()
+    return rec
+
+
 def main(argv=None) -> int:
-    ap = argparse.ArgumentParser(description="Train the warm-start surrogate on the seeded channel sweep.")
-    ap.add_argument("command", choices=["train"])
-    ap.add_argument("--out", required=True)
-    ap.add_argument("--cases", type=int, default=200)
+    ap = argparse.ArgumentParser(description="Warm-start surrogates: train on the seeded channel sweep, or time "
+                                             "the swept wing's drop with and without one.")
+    ap.add_argument("command", choices=["train", "wing"])
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--cases", type=int, default=None)
     ap.add_argument("--steps", type=int, default=40000)
     a = ap.parse_args(argv)
-    info = train_warmstart(a.out, n_cases=a.cases, steps=a.steps)
+    if a.command == "train":
+        if not a.out:
+            ap.error("train needs --out")
+        info = train_warmstart(a.out, n_cases=a.cases or 200, steps=a.steps)
+    else:
+        info = wing_warmstart(n_train=a.cases or 32, out=a.out)
     print(json.dumps(info))
     return 0
 
