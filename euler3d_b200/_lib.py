@@ -21,7 +21,7 @@ ERRORS = {
 GRAD = {"greengauss": 0, "leastsquares": 1}
 LIM = {"barthjespersen": 0, "venkatakrishnan": 1}
 FLUX = {"roe": 0, "ausm": 1}
-FP64, FP32, FP64_FMA = 0, 1, 2
+FP64, FP32, FP64_FMA, FP32_DELTA = 0, 1, 2, 3
 # e3d_options.renumber: a base order, optionally "+boundary_last" (cells with a ghost neighbour last)
 RENUMBER = {f"{k}{suffix}": v + flag for k, v in {"none": 0, "rcm": 1, "morton": 2, "shuffle": 3}.items()
             for suffix, flag in (("", 0), ("+boundary_last", 16))}

@@ -263,11 +263,13 @@ class Batch(Solver):
 
 
 def set_precision(solver: Solver, precision: str) -> None:
-    """Switch an FP32 solver (or batch) to FP64 in place: "fp64", or "fp64-fma" for batch
-    solves with the FP64 kernels built with fused multiply-add."""
-    code = {"fp64": L.FP64, "fp64-fma": L.FP64_FMA, "fp32": L.FP32}[precision]
+    """Switch an FP32 solver (or batch) in place: to FP64 ("fp64", or "fp64-fma" for batch
+    solves with the FP64 kernels built with fused multiply-add), or to "fp32-delta", FP32
+    batch solves in difference form (an FP64 base state and FP32 differences, the base
+    residual in FP64), which fall below the FP32 floor (first-order AUSM, tetrahedra)."""
+    code = {"fp64": L.FP64, "fp64-fma": L.FP64_FMA, "fp32": L.FP32, "fp32-delta": L.FP32_DELTA}[precision]
     L.check(L.lib().e3d_solver_set_precision(solver._h, code))
-    solver.precision = "fp32" if precision == "fp32" else "fp64"
+    solver.precision = precision if precision in ("fp32", "fp32-delta") else "fp64"
 
 
 def cell_features(solver: Solver) -> np.ndarray:

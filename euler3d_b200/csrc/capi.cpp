@@ -407,8 +407,10 @@ int e3d_solver_set_precision(e3d_solver* s, int precision) {
 		if (precision == E3D_FP64 || precision == E3D_FP64_FMA) {
 			eng(s).widen_to_fp64();
 			eng(s).set_fp64_contracted(precision == E3D_FP64_FMA);
+		} else if (precision == E3D_FP32_DELTA) {
+			eng(s).enter_delta();
 		} else if (precision != E3D_FP32 || eng(s).precision() != e3d::PREC_FP32) {
-			throw e3d::Error(E3D_ERR_ARG, "a solver switches from FP32 to FP64 only");
+			throw e3d::Error(E3D_ERR_ARG, "a solver switches from FP32 to FP64 or to the FP32 difference form only");
 		}
 	});
 }

@@ -681,6 +681,7 @@ static ReduceArgs make_reduce(int NR, int NA, int nb, const int* roff, int chunk
 }
 
 void Engine::flow_data(std::vector<double>& out) {
+	require_not_delta("flow_data");
 	ReduceArgs a = make_reduce(NR_, NA_, nb_, roff_d_.p, chunk_, max_chunks_, partial_.p, wall_off_.p, wall_face_.p,
 	                           (int)wall_face_.n, wall_terms_.p, face_lr_.p, S_.p, fc_.p, denom_, fd_hist_.p, zero_d_.p,
 	                           bad_d_.p);
@@ -831,6 +832,7 @@ void Engine::require_exchanged(int n_iter) const {
 }
 
 void Engine::iterate(int n) {
+	require_not_delta("iterate");
 	if (n < 0) throw Error(E3D_ERR_ARG, "negative iteration count");
 	require_exchanged(n);
 	if (!started_) halo();  // Solver.cpp:48, before the first iteration
@@ -839,6 +841,7 @@ void Engine::iterate(int n) {
 }
 
 double Engine::iterate_timed(int n) {
+	require_not_delta("iterate_timed");
 	if (n < 0) throw Error(E3D_ERR_ARG, "negative iteration count");
 	require_exchanged(n);
 	if (!started_) halo();
@@ -898,6 +901,7 @@ size_t Engine::state_bytes() const {
 // Layout: header, then primitives [5][NA] in device order (real cells of every
 // block, then ghost cells of every block) and precision, then FP64 W0 [5][NR].
 void Engine::export_state(void* host, size_t bytes) {
+	require_not_delta("export_state");
 	if (!host || bytes < state_bytes()) throw Error(E3D_ERR_ARG, "state buffer too small");
 	StateHeader h{};
 	std::memcpy(h.magic, "E3DSTAT1", 8);
@@ -921,6 +925,7 @@ void Engine::export_state(void* host, size_t bytes) {
 }
 
 void Engine::import_state(const void* host, size_t bytes) {
+	require_not_delta("import_state");
 	if (!host || bytes < sizeof(StateHeader)) throw Error(E3D_ERR_ARG, "state buffer too small");
 	StateHeader h;
 	std::memcpy(&h, host, sizeof(h));
@@ -1072,6 +1077,7 @@ void Engine::collect_history(int first_iter, int n) {
 }
 
 int Engine::solve(int max_iter, double criterion, int check_every) {
+	require_not_delta("solve");
 	if (shard_)
 		throw Error(E3D_ERR_STATE, "a shard's stop test needs the norms of every rank: iterate, exchange and push "
 		                           "the gathered flow data instead");
@@ -1203,8 +1209,14 @@ void Engine::get(const std::string& name, int b, std::vector<double>& out) {
 		d2h_packed(dev, NA_, g0, ng, out, nr, na, st_);
 		to_local(b, out, 5, na);
 	};
+	if (delta_ && name != "prim" && name != "w0") throw Error(E3D_ERR_STATE, "only prim and w0 are readable in difference form");
+	if (delta_) {
+		rebase();  // differences folded into the base: base = full state
+		cuda_ok(cudaStreamSynchronize(st_), "sync");
+	}
 	if (name == "prim") {
-		if (f64) packed_all(cur_ ? f64_.P1.p : f64_.P0.p);
+		if (delta_) packed_all(Pb64_.p);
+		else if (f64) packed_all(cur_ ? f64_.P1.p : f64_.P0.p);
 		else packed_all(cur_ ? f32_.P1.p : f32_.P0.p);
 	} else if (name == "conv_res") {
 		if (f64) rows_real(5, f64_.Rc.p);
@@ -1239,6 +1251,7 @@ void Engine::get(const std::string& name, int b, std::vector<double>& out) {
 }
 
 void Engine::set(const std::string& name, int b, const std::vector<double>& in_local) {
+	require_not_delta("set");
 	if (b < 0 || b >= nb_) throw Error(E3D_ERR_ARG, "block index out of range");
 	cuda_ok(cudaStreamSynchronize(st_), "sync");
 	const int nr = n_real_b_[b], na = n_all_b_[b], ng = na - nr, r0 = roff_[b], g0 = NR_ + goff_[b];
@@ -1338,6 +1351,7 @@ double Engine::bytes_flux(bool order1, bool diss, bool last) const {
 }
 
 std::vector<Engine::KernelTime> Engine::time_kernels(int n) {
+	require_not_delta("time_kernels");
 	if (deck_.smoothing) throw Error(E3D_ERR_STATE, "per-kernel timing covers the fused path (no residual smoothing)");
 	std::vector<KernelTime> out;
 	if (!started_) halo();
@@ -1518,13 +1532,24 @@ double Engine::run_persistent_t(int iters) {
 		v.W0 = W0_.p;
 		v.case_free = ncases_ > 1 ? case_free_d_.p : nullptr;  // single case: Physics::free
 		v.gcase = gcase_d_.p;
+		if (delta_) {
+			v.Pb = Pb32_.p;
+			v.Pb64 = Pb64_.p;
+			v.dW = dW_.p;
+			v.Rb = Rb_.p;
+			v.slot_face = slot_face_.p;
+			v.nhat64 = nhat_.p;
+		}
 		return v;
 	};
+	a.Pb64 = delta_ ? Pb64_.p : nullptr;
 	const FusedView<T> v0 = view(false), v1 = view(true);
 	const int grid = tiled_ ? n_work_ : std::max(1, std::min(grid_, n_work_));
 	const bool fast = std::is_same<T, double>::value && fast64_;
 	auto launch = [&]() {
 		const bool o2 = order_ == 2;
+		if constexpr (std::is_same<T, float>::value)
+			if (delta_) return delta::launch_iterations(v0, v1, ph_, a, st_);
 		if (fast)
 			return tiled_ ? batch_fast::launch_tiled_iterations<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, o2, st_)
 			              : batch_fast::launch_persistent<T>(v0, v1, ph_, a, grad_kind_, lim_kind_, scheme_, o2, grid, st_);
@@ -1741,6 +1766,7 @@ double Engine::solve_batch(int max_iter, double criterion, int iters_per_launch,
 				room = std::min(room, max_iter - (int)hist_case_[c].size());
 			}
 		if (!any || room <= 0) break;
+		if (delta_) rebase();  // device work on the stream, counted in the launch's time below
 		ms_total += run_persistent(std::min(iters_per_launch, room));
 		const auto n_failed = [&]() { return std::count(case_failed_.begin(), case_failed_.end(), 1); };
 		const auto failed_before = n_failed();
@@ -1777,6 +1803,7 @@ void Engine::cell_features(float* dev_out) {
 }
 
 void Engine::conservative_rows(float* dev_out) {
+	require_not_delta("conservative_rows");
 	if (opt_.precision == PREC_FP32)
 		launch_prims_to_conservative<float>(NR_, NA_, cur_ ? f32_.P1.p : f32_.P0.p, ph_.gamma, dev_out, st_);
 	else
@@ -1785,6 +1812,7 @@ void Engine::conservative_rows(float* dev_out) {
 }
 
 int Engine::apply_conservative(const float* dev_w, int ld) {
+	require_not_delta("apply_conservative");
 	if (ld < 5) throw Error(E3D_ERR_ARG, "conservative rows need at least 5 columns");
 	cuda_ok(cudaMemsetAsync(fallback_d_.p, 0, sizeof(int), st_), "memset");
 	if (opt_.precision == PREC_FP32)
@@ -1816,6 +1844,7 @@ void Engine::set_fp64_contracted(bool on) {
 
 void Engine::widen_to_fp64() {
 	if (opt_.precision == PREC_FP64) return;
+	if (delta_) leave_delta();
 	cuda_ok(cudaStreamSynchronize(st_), "sync");
 	const bool need_gg = order_ == 2 && grad_kind_ == GRAD_GREEN_GAUSS;
 	const bool need_ls = order_ == 2 && grad_kind_ == GRAD_LEAST_SQUARES;
@@ -1866,6 +1895,107 @@ void Engine::widen_to_fp64() {
 	grid_ = 0;
 	tuning_ = Tuning{};
 	snap_.free();
+	count_device_bytes();
+}
+
+// ---------------------------------------------------------------- difference form
+void Engine::require_not_delta(const char* what) const {
+	if (delta_)
+		throw Error(E3D_ERR_STATE, std::string(what) + ": the solver runs batch solves in difference form");
+}
+
+FusedView<float> Engine::delta_view(bool flip) const {
+	FusedView<float> v = f32_.view(flip);
+	v.NR = NR_;
+	v.NG = NG_;
+	v.NA = NA_;
+	v.NS = NS_;
+	v.tet4 = tet4_;
+	v.slot_ptr = slot_ptr_.p;
+	v.slot_nbr = slot_nbr_.p;
+	v.slot_mate = slot_mate_.p;
+	v.gkind = gkind_.p;
+	v.grefl = grefl_.p;
+	v.W0 = W0_.p;
+	v.case_free = ncases_ > 1 ? case_free_d_.p : nullptr;
+	v.gcase = gcase_d_.p;
+	v.Pb = Pb32_.p;
+	v.Pb64 = Pb64_.p;
+	v.dW = dW_.p;
+	v.Rb = Rb_.p;
+	v.slot_face = slot_face_.p;
+	v.nhat64 = nhat_.p;
+	return v;
+}
+
+// W_b <- W_b + dW, base primitives and ghosts from it, base residual in FP64,
+// differences cleared (both primitive buffers)
+void Engine::rebase() {
+	delta::launch_rebase(delta_view(false), ph_, W0_.p, area_.p, (int)halo_dst_.n, halo_dst_.p, halo_src_.p, f32_.P0.p,
+	                     f32_.P1.p, st_);
+	check("rebase");
+}
+
+void Engine::enter_delta() {
+	if (delta_) return;
+	if (opt_.precision != PREC_FP32) throw Error(E3D_ERR_STATE, "the difference form starts from an FP32 solver");
+	if (order_ != 1 || scheme_ != FLUX_AUSM)
+		throw Error(E3D_ERR_ARG, "the difference form covers first-order AUSM");
+	if (!tet4_) throw Error(E3D_ERR_ARG, "the difference form covers all-tetrahedron meshes");
+	if (!carry_) throw Error(E3D_ERR_STATE, "the difference form needs the carried FP64 state");
+	if (shard_) throw Error(E3D_ERR_STATE, "the difference form runs on a whole case, not on a shard");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	Pb32_.alloc(5 * (size_t)NA_);
+	Pb64_.alloc(5 * (size_t)NA_);
+	dW_.alloc(5 * (size_t)NR_);
+	Rb_.alloc(5 * (size_t)NR_);
+	// every cell's base from the current state (real cells from the carried W,
+	// others from the FP32 primitives: ghosts that no condition or halo rewrites)
+	launch_widen_state(NA_, NR_, cur_ ? f32_.P1.p : f32_.P0.p, W0_.p, ph_.gm1, Pb64_.p, nullptr, st_);
+	launch_narrow_state(NA_, Pb64_.p, Pb32_.p, st_);
+	cuda_ok(cudaMemsetAsync(dW_.p, 0, dW_.n * sizeof(float), st_), "memset");
+	cuda_ok(cudaMemsetAsync(f32_.P0.p, 0, f32_.P0.n * sizeof(float), st_), "memset");
+	cuda_ok(cudaMemsetAsync(f32_.P1.p, 0, f32_.P1.n * sizeof(float), st_), "memset");
+	check("enter difference form");
+	delta_ = true;
+	rebase();
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	if (pgraph_) {
+		cudaGraphExecDestroy(pgraph_);
+		pgraph_ = nullptr;
+	}
+	for (auto& g : graph_)
+		if (g) {
+			cudaGraphExecDestroy(g);
+			g = nullptr;
+		}
+	// one form: tiles of 128 cells, per-pass launches in a graph (no autotuning)
+	tiled_ = true;
+	tile_mult_ = 1;
+	grid_ = 1;
+	tuning_ = Tuning{};
+	tuning_.tile_cells = kPersistThreads;
+	tuning_.tiled = true;
+	snap_.free();
+	count_device_bytes();
+}
+
+// back to the plain FP32 form: fold the differences into the base and write the
+// base primitives (FP32) into both buffers; W0_ holds the full FP64 state
+void Engine::leave_delta() {
+	rebase();
+	cuda_ok(cudaMemcpyAsync(f32_.P0.p, Pb32_.p, Pb32_.n * sizeof(float), cudaMemcpyDeviceToDevice, st_), "d2d");
+	cuda_ok(cudaMemcpyAsync(f32_.P1.p, Pb32_.p, Pb32_.n * sizeof(float), cudaMemcpyDeviceToDevice, st_), "d2d");
+	cuda_ok(cudaStreamSynchronize(st_), "sync");
+	for (auto* b : {&Pb32_, &dW_, &Rb_}) b->free();
+	Pb64_.free();
+	delta_ = false;
+	if (pgraph_) {
+		cudaGraphExecDestroy(pgraph_);
+		pgraph_ = nullptr;
+	}
+	grid_ = 0;
+	tuning_ = Tuning{};
 	count_device_bytes();
 }
 

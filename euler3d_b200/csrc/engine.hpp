@@ -168,6 +168,13 @@ public:
 	// differences from the bit-identical FP64 path); affects e3d_batch_solve only
 	void set_fp64_contracted(bool on);
 	bool fp64_contracted() const { return fast64_; }
+	// FP32 solver -> FP32 iterations in difference form (delta.cu) for batch
+	// solves: first-order AUSM on all-tetrahedron meshes.  The state is an FP64
+	// base (rebased before every batch launch, with its residual evaluated in
+	// FP64) plus FP32 differences, so the residual falls below the FP32 floor.
+	// widen_to_fp64 leaves the form; get("prim") returns the full state.
+	void enter_delta();
+	bool delta() const { return delta_; }
 	long long n_real_case(int c) const;
 	void sync();  // waits for queued work; throws on a CUDA error or a non-finite norm
 
@@ -296,6 +303,15 @@ private:
 	void snapshot(bool save);
 	DevBuf<unsigned char> snap_;
 	DevBuf<double> irs_;  // residual-smoothing Jacobi start values, 10 x NR
+	// difference form: base primitives (FP32 copy and FP64), carried conserved
+	// differences, base residual; W0_ holds the FP64 base conserved state
+	bool delta_ = false;
+	DevBuf<float> Pb32_, dW_, Rb_;
+	DevBuf<double> Pb64_;
+	FusedView<float> delta_view(bool flip) const;
+	void rebase();
+	void leave_delta();
+	void require_not_delta(const char* what) const;
 	size_t dev_bytes_ = 0;
 };
 

@@ -904,8 +904,12 @@ template <class T>
 __device__ __forceinline__ void wall_terms_range(const FusedView<T>& vf, const PersistArgs& a, int i0, int stride) {
 	for (int i = i0; i < a.n_wall; i += stride) {
 		const int f = a.wall_face[i];
-		const double p0 = (double)vf.Pin[4 * (size_t)vf.NA + a.face_lr[2 * f]];
-		const double p1 = (double)vf.Pin[4 * (size_t)vf.NA + a.face_lr[2 * f + 1]];
+		const size_t i0 = 4 * (size_t)vf.NA + a.face_lr[2 * f], i1 = 4 * (size_t)vf.NA + a.face_lr[2 * f + 1];
+		double p0 = (double)vf.Pin[i0], p1 = (double)vf.Pin[i1];
+		if (a.Pb64) {  // difference form: base + difference
+			p0 += a.Pb64[i0];
+			p1 += a.Pb64[i1];
+		}
 		const double cp = (0.5 * (p0 + p1) - 1.) / (a.wall_denom ? a.wall_denom[i] : a.denom);
 		const double fx = cp * a.S[3 * f], fy = cp * a.S[3 * f + 1], fz = cp * a.S[3 * f + 2];
 		const double x = a.fc[3 * f], y = a.fc[3 * f + 1], z = a.fc[3 * f + 2];

@@ -93,6 +93,17 @@ cudaError_t launch_tiled_iterations(const FusedView<T>& v0, const FusedView<T>& 
                                     const PersistArgs& a, int grad, int lim, int scheme, bool order2, cudaStream_t st);
 }  // namespace batch_fast
 
+// FP32 iterations in difference form (delta.cu): first-order AUSM, all-tetrahedron
+// meshes, tiled per-pass form.  v0/v1 carry the base and difference arrays.
+namespace delta {
+cudaError_t launch_iterations(const FusedView<float>& v0, const FusedView<float>& v1, const Physics& ph,
+                              const PersistArgs& a, cudaStream_t st);
+// new base state from W_b + dW (Wb: the FP64 base conserved state, updated in
+// place), base ghosts, base residual in FP64; differences d0, d1 cleared
+void launch_rebase(const FusedView<float>& v, const Physics& ph, double* Wb, const double* area64, int n_halo,
+                   const int* halo_dst, const int* halo_src, float* d0, float* d1, cudaStream_t st);
+}  // namespace delta
+
 template <class T>
 void launch_flux_update(const FusedView<T>&, const Physics&, int scheme, bool order1, double alpha, double beta,
                         int last, int carry, cudaStream_t);

@@ -78,6 +78,15 @@ struct FusedView {
 	T* dt;                  // NR
 	const double* case_free;  // 5 per case, or null: every ghost uses Physics::free
 	const int* gcase;         // NG case index of each ghost (with case_free)
+	// difference form (delta.cu; null otherwise): Pin/Pout hold differences from
+	// the base primitives Pb (FP32 copy of Pb64), dW the carried conserved
+	// differences from the FP64 base W_b, Rb the FP64-evaluated base residual
+	const float* Pb;          // 5*NA
+	const double* Pb64;       // 5*NA
+	float* dW;                // 5*NR
+	float* Rb;                // 5*NR
+	const int* slot_face;     // NS  (FP64 face normals of boundary slots)
+	const double* nhat64;     // 3*NF
 };
 
 // One launch of the persistent batch kernel: several outer iterations over the
@@ -113,6 +122,8 @@ struct PersistArgs {
 	int n_halo;
 	const int* halo_dst;
 	const int* halo_src;
+	// difference form: FP64 base primitives (wall pressures are base + difference), else null
+	const double* Pb64;
 };
 
 }  // namespace e3d

@@ -52,12 +52,17 @@ __global__ void k_widen_state(int NA, int NR, const float* __restrict__ P32, con
 		for (int v = 0; v < 4; v++) q[v] = (double)P32[4 * (size_t)c + v];
 		q[4] = (double)P32[4 * (size_t)NA + c];
 	}
-	for (int v = 0; v < 4; v++) {
-		P0[4 * (size_t)c + v] = q[v];
-		P1[4 * (size_t)c + v] = q[v];
-	}
+	for (int v = 0; v < 4; v++) P0[4 * (size_t)c + v] = q[v];
 	P0[4 * (size_t)NA + c] = q[4];
-	P1[4 * (size_t)NA + c] = q[4];
+	if (P1) {
+		for (int v = 0; v < 4; v++) P1[4 * (size_t)c + v] = q[v];
+		P1[4 * (size_t)NA + c] = q[4];
+	}
+}
+
+__global__ void k_narrow_state(size_t n, const double* __restrict__ P64, float* __restrict__ P32) {
+	const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (i < n) P32[i] = (float)P64[i];
 }
 
 __global__ void k_cell_features(int NR, int nb, const int* __restrict__ roff, const int* __restrict__ block_case,
@@ -161,6 +166,10 @@ void launch_slot_geometry64(int NS, const int* slot_face, const int* slot_mate, 
 void launch_widen_state(int NA, int NR, const float* P32, const double* W, double gm1, double* P0, double* P1,
                         cudaStream_t st) {
 	if (NA > 0) k_widen_state<<<grid_for(NA), TPB, 0, st>>>(NA, NR, P32, W, gm1, P0, P1);
+}
+
+void launch_narrow_state(int NA, const double* P64, float* P32, cudaStream_t st) {
+	if (NA > 0) k_narrow_state<<<grid_for(5LL * NA), TPB, 0, st>>>(5 * (size_t)NA, P64, P32);
 }
 
 void launch_cell_features(int NR, int nb, const int* roff, const int* block_case, const float* centroid,

@@ -13,11 +13,15 @@ void launch_slot_geometry64(int NS, const int* slot_face, const int* slot_mate, 
                             const double* area, const double* rl, const double* rr, double* sgeo, double* sS,
                             double* srv, cudaStream_t st);
 
-// FP64 copy of an FP32 packed primitive state, into both ping-pong buffers.
+// FP64 copy of an FP32 packed primitive state, into both ping-pong buffers
+// (only P0 when P1 is null).
 // With W (the carried FP64 conservative state, [5][NR]) the real cells are
 // recomputed from it exactly; ghost cells are widened from P32.
 void launch_widen_state(int NA, int NR, const float* P32, const double* W, double gm1, double* P0, double* P1,
                         cudaStream_t st);
+
+// FP32 copy of an FP64 packed primitive state (all NA cells)
+void launch_narrow_state(int NA, const double* P64, float* P32, cudaStream_t st);
 
 // Raw surrogate inputs of every real cell, [NR][8] floats:
 // x, y, z (centroid), distance to the nearest wall-face centre of the cell's

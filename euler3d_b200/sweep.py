@@ -92,8 +92,9 @@ def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrog
     iterations to `switch_at` (below a 4-order drop, a case whose FP32
     residual has stopped falling for `stall_window` iterations, its FP32
     rounding floor, also moves on),
-    then FP64 iterations to `criterion` (`fp64`: "fp64-fma" for the kernels
-    built with fused multiply-add, "fp64" for the bit-identical ones); each
+    then the finishing phase to `criterion` (`fp64`: "fp64-fma" for the FP64
+    kernels built with fused multiply-add, "fp64" for the bit-identical ones,
+    "fp32-delta" for FP32 iterations in difference form on an FP64 base); each
     case leaves the work list once it gets there."""
     t0 = time.perf_counter()
     b = api.Batch(cases, precision="fp32" if switch_at is not None else "fp64",
@@ -122,7 +123,8 @@ def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrog
         phases.append(dict(precision="switch", wall_s=time.perf_counter() - tp))
     tp = time.perf_counter()
     b.solve_batch(max_iter, criterion, iters_per_launch=iters_per_launch)
-    phases.append(dict(precision="fp64", to=criterion, wall_s=time.perf_counter() - tp, tuning=b.tuning()))
+    phases.append(dict(precision=fp64 if switch_at is not None else "fp64", to=criterion,
+                       wall_s=time.perf_counter() - tp, tuning=b.tuning()))
     wall = time.perf_counter() - t0
     per_case = []
     for c in range(len(cases)):
@@ -268,10 +270,60 @@ def wing_warmstart(n_train: int = 32, train_dims=(64, 20, 24, 8), target_dims=(1
     return rec
 
 
+def finishing_forms(n: int = 48, count: int = 8, iters: int = 300, depth_cases: int = 2,
+                    depth: float = -11.0) -> dict:
+    """The finishing phase's three forms on one batch of `count` channel cases
+    (n^3 x 6 tets each, first-order AUSM, per-pass form for all three): device
+    ms per iteration of FP32, FP32 in difference form and FP64 with
+    contraction, each after 100 warm-up iterations; then `depth_cases` of them
+    from freestream to `depth`, once in contracted FP64 and once FP32 to -5
+    followed by the difference form (iterations needed, converged Cl/Cd)."""
+    import tempfile
+
+    specs = polar_specs(HELD_OUT_SEED, count, n_range=(n, n), prefix="test")
+    rec = dict(n=n, cases=count, iters=iters, scheme=WARM_SCHEME, forms={})
+    old_form = os.environ.get("E3D_BATCH_FORM")
+    os.environ["E3D_BATCH_FORM"] = "per-pass"
+    try:
+        with tempfile.TemporaryDirectory() as td:
+            cases = [api.Case(d) for d in write_cases(td, specs, WARM_SCHEME, sides="channel")]
+            cells = sum(c.block_info(b).n_real for c in cases for b in range(c.n_blocks))
+            rec["cells"] = cells
+            b = api.Batch(cases, precision="fp32", hist_capacity=4096)
+            it = 1
+            b.solve_batch(it, -1e300, iters_per_launch=1)
+            for form in ("fp32", "fp32-delta", "fp64-fma"):
+                if form != "fp32":
+                    api.set_precision(b, form)
+                it += 100
+                b.solve_batch(it, -1e300, iters_per_launch=50)
+                it += iters
+                _, ms = b.solve_batch(it, -1e300, iters_per_launch=100)
+                rec["forms"][form] = dict(ms_per_iter=ms / iters, cell_iters_per_s=cells * iters / (ms / 1e3))
+            b.close()
+            sub = cases[:depth_cases]
+            a = solve_batched(sub, depth, 200000, switch_at=None, fp64="fp64-fma")
+            d = solve_batched(sub, depth, 200000, switch_at=-5.0, fp64="fp32-delta")
+            rec["depth"] = dict(level=depth, fp64_fma=a, fp32_then_delta=d,
+                                max_rel_dcl=max(abs(x["cl"] - y["cl"]) / abs(y["cl"])
+                                                for x, y in zip(d["cases"], a["cases"])),
+                                max_rel_dcd=max(abs(x["cd"] - y["cd"]) / abs(y["cd"])
+                                                for x, y in zip(d["cases"], a["cases"])))
+            for c in cases:
+                c.close()
+    finally:
+        if old_form is None:
+            os.environ.pop("E3D_BATCH_FORM", None)
+        else:
+            os.environ["E3D_BATCH_FORM"] = old_form
+    return rec
+
+
 def main(argv=None) -> int:
-    ap = argparse.ArgumentParser(description="Warm-start surrogates: train on the seeded channel sweep, or time "
-                                             "the swept wing's drop with and without one.")
-    ap.add_argument("command", choices=["train", "wing"])
+    ap = argparse.ArgumentParser(description="Warm-start surrogates: train on the seeded channel sweep, time "
+                                             "the swept wing's drop with and without one, or time the finishing "
+                                             "phase's forms.")
+    ap.add_argument("command", choices=["train", "wing", "finishing"])
     ap.add_argument("--out", default=None)
     ap.add_argument("--cases", type=int, default=None)
     ap.add_argument("--steps", type=int, default=40000)
@@ -280,8 +332,10 @@ def main(argv=None) -> int:
         if not a.out:
             ap.error("train needs --out")
         info = train_warmstart(a.out, n_cases=a.cases or 200, steps=a.steps)
-    else:
+    elif a.command == "wing":
         info = wing_warmstart(n_train=a.cases or 32, out=a.out)
+    else:
+        info = finishing_forms(count=a.cases or 8)
     print(json.dumps(info))
     return 0
 

@@ -43,6 +43,7 @@ extern "C" {
 #define E3D_FP64 0 /* drop-in: reference FP64 arithmetic */
 #define E3D_FP32 1 /* FP32 bulk, FP64 conserved state and reductions */
 #define E3D_FP64_FMA 2 /* e3d_solver_set_precision only: FP64, batch solves with fused multiply-add */
+#define E3D_FP32_DELTA 3 /* e3d_solver_set_precision only: FP32 batch solves in difference form (below) */
 
 typedef struct e3d_case e3d_case;     /* host case: deck + topology + blocks */
 typedef struct e3d_solver e3d_solver; /* device-resident solver over one case */
@@ -270,7 +271,17 @@ int e3d_shard_push_flow_data(e3d_solver* s, const double* all_blocks, int n_iter
  * multiply-add: the same discrete equations and converged solution, not
  * bit-identical to the reference (E3D_FP64 switches an FP64 solver back).  The FP32 path's
  * residual stops dropping near 5 orders (FP32 rounding of the fluxes); a run
- * to a deeper drop continues in FP64 from there.
+ * to a deeper drop continues in FP64 from there, or with E3D_FP32_DELTA in
+ * FP32 difference form: the state becomes an FP64 base plus FP32 differences,
+ * the base and its residual (FP64) are renewed before every batch launch of
+ * e3d_batch_solve, and the per-stage residual is the FP64 base residual plus
+ * the change of the fluxes since the base, evaluated in FP32 in a form whose
+ * rounding scales with that change.  The residual then keeps falling below the
+ * FP32 floor at FP32 cost, to the FP64 path's converged state (not bit for bit).
+ * First-order AUSM on all-tetrahedron meshes; E3D_ERR_ARG otherwise.  In this
+ * form only e3d_batch_solve, e3d_history / e3d_batch_case_history, reading
+ * "prim" and "w0" (the full state), and a further switch to E3D_FP64 or
+ * E3D_FP64_FMA are available; other calls return E3D_ERR_STATE.
  * e3d_cell_features: surrogate inputs of every real cell of every case, in
  * device cell order (blocks in order, real cells in the order that
  * e3d_options.renumber chose; file order by default), 8 floats per
