@@ -644,6 +644,111 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? E3D_RECON_MIN_BLOCKS : E
 	if (c < v.NR) recon_cell<T, GRAD, LIM, FIRST, NSL>(v, ph, carry_w0, c);
 }
 
+// FP64 reconstruction of the later stages with one lane per (cell, variable),
+// all-tetrahedron meshes.  Gradient, limiter and face states of one variable
+// depend on that variable alone, so five lanes per cell run the same
+// per-variable arithmetic as recon_cell's FP64 branch, in the same order (bit
+// for bit), with a fifth of its gradient/limiter state and the slot weights
+// read per slot: 64 registers instead of 128, 30 resident warps per SM instead
+// of 16.  A block covers RV_CELLS cells (5 * RV_CELLS threads, cell-major: the
+// four lanes of a cell's (rho, u, v, w) read and write one 32-byte vector
+// together).  Measured on B200 (3.07M tets, second order): 2.61 TB/s against
+// 2.44 for the one-thread-per-cell pass.  The first stage keeps recon_cell: its
+// time step and W0 need the whole cell, and one lane of five doing them made
+// that pass slower (2.82 against 2.89 TB/s).
+constexpr int RV_CELLS = 32;
+#ifndef E3D_RV_MIN_BLOCKS
+#define E3D_RV_MIN_BLOCKS 6
+#endif
+
+__device__ __forceinline__ double ldq(const double* __restrict__ P, int n, int c, int q) {
+	return q < 4 ? P[4 * (size_t)c + q] : P[4 * (size_t)n + c];
+}
+__device__ __forceinline__ void stq(double* __restrict__ P, int n, int c, int q, double x) {
+	if (q < 4) P[4 * (size_t)c + q] = x;
+	else P[4 * (size_t)n + c] = x;
+}
+
+template <int GRAD, int LIM>
+__global__ void __launch_bounds__(5 * RV_CELLS, E3D_RV_MIN_BLOCKS) k_recon_var(FusedView<double> v, Physics ph) {
+	const int c = blockIdx.x * RV_CELLS + threadIdx.x / 5, q = threadIdx.x % 5;
+	if (c >= v.NR) return;
+	const SlotRange<double, 4> sr(v, c);
+	const double q0 = ldq(v.Pin, v.NA, c, q);
+	int nb[4];
+	load_int<double, 4>(v.slot_nbr, sr, nb);
+	double gr[3] = {0.0, 0.0, 0.0};
+	double mx = q0, mn = q0;
+	{
+		const double* __restrict__ wa = (GRAD == GRAD_GREEN_GAUSS ? v.sS : v.lsw) + 3 * (size_t)sr.s0;
+#pragma unroll
+		for (int k = 0; k < 4; k++) {
+			const double w[1][3] = {{__ldg(wa + 3 * k), __ldg(wa + 3 * k + 1), __ldg(wa + 3 * k + 2)}};
+			const double qn = ldq(v.Pin, v.NA, nb[k], q);
+			if (GRAD == GRAD_GREEN_GAUSS) {
+				const double a = 0.5 * (q0 + qn);
+				gr[0] += a * w[0][0];
+				gr[1] += a * w[0][1];
+				gr[2] += a * w[0][2];
+			} else {
+				const double dq = qn - q0;
+				gr[0] += w[0][0] * dq;
+				gr[1] += w[0][1] * dq;
+				gr[2] += w[0][2] * dq;
+			}
+			if (qn > mx) mx = qn;
+			if (qn < mn) mn = qn;
+		}
+	}
+	const double V = v.vol[c];
+	if (GRAD == GRAD_GREEN_GAUSS)
+		for (int d = 0; d < 3; d++) gr[d] /= V;
+	const double* __restrict__ ra = v.srv + 3 * (size_t)sr.s0;
+	const double eps2 = ph.k3 * V;
+	const double dmax = mx - q0, dmin = mn - q0;
+	double phi = INFINITY;
+#pragma unroll
+	for (int k = 0; k < 4; k++) {
+		double d2 = 0.0;
+		d2 += gr[0] * __ldg(ra + 3 * k);
+		d2 += gr[1] * __ldg(ra + 3 * k + 1);
+		d2 += gr[2] * __ldg(ra + 3 * k + 2);
+		const double lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2, dmax, dmin, ph.omega)
+		                                               : limiter_venkat_face(d2, dmax, dmin, eps2);
+		if (lf < phi) phi = lf;
+	}
+#pragma unroll
+	for (int k = 0; k < 4; k++)
+		stq(v.FS, v.NS, sr.s0 + k, q,
+		    recon(q0, phi, gr[0], gr[1], gr[2], __ldg(ra + 3 * k), __ldg(ra + 3 * k + 1), __ldg(ra + 3 * k + 2)));
+	// ghost cells of this cell's boundary faces (recon_cell's tail, one variable)
+#pragma unroll
+	for (int k = 0; k < 4; k++) {
+		if (nb[k] < v.NR) continue;
+		const int g = nb[k];
+		int ms = v.slot_mate[sr.s0 + k];
+		ms = ms >= 0 ? ms : ~ms;
+		const double qg = ldq(v.Pin, v.NA, g, q);
+		const double* n = v.sgeo + 4 * (size_t)(sr.s0 + k);
+		const double g0 = v.srv[3 * (size_t)ms], g1 = v.srv[3 * (size_t)ms + 1], g2 = v.srv[3 * (size_t)ms + 2];
+		double gg[3] = {0.0, 0.0, 0.0};
+		if (v.grefl[g - v.NR] != 0) reflect_grad(gr, n[0], n[1], n[2], gg);
+		double gmx = qg, gmn = qg;
+		if (q0 > gmx) gmx = q0;
+		if (q0 < gmn) gmn = q0;
+		double d2 = 0.0;
+		d2 += gg[0] * g0;
+		d2 += gg[1] * g1;
+		d2 += gg[2] * g2;
+		const double dmx = gmx - qg, dmn = gmn - qg;
+		const double lf = (LIM == LIM_BARTH_JESPERSEN) ? limiter_bj_face(d2, dmx, dmn, ph.omega)
+		                                               : limiter_venkat_face(d2, dmx, dmn, ph.k3 * v.vol[g]);
+		double pg = INFINITY;
+		if (lf < pg) pg = lf;
+		stq(v.FS, v.NS, ms, q, recon(qg, pg, gg[0], gg[1], gg[2], g0, g1, g2));
+	}
+}
+
 // W0 and the local time step without a reconstruction pass (first order).
 template <class T, int NSL>
 __device__ __forceinline__ void start_cell(const FusedView<T>& v, const Physics& ph, int carry_w0, int c) {

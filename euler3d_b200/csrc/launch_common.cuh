@@ -33,9 +33,20 @@ void launch_reduce(const ReduceArgs& a, const T* Rc, const T* Rd, const T* P, cu
 	k_wall_sums<<<a.nblocks, 128, 0, st>>>(a.wall_terms, a.n_wall, a.wall_off, a.hist, a.stride, a.d_iter);
 }
 
+// FP64 later stages on tetrahedra: one lane per (cell, variable)
+// (k_recon_var); build with -DE3D_FP64_RECON_VAR=0 for the one-thread-per-cell pass
+#ifndef E3D_FP64_RECON_VAR
+#define E3D_FP64_RECON_VAR 1
+#endif
 template <class T, int GRAD, int LIM>
 void recon_dispatch_first(const FusedView<T>& v, const Physics& ph, bool first, int carry, cudaStream_t st) {
 	const int grid = (v.NR + 127) / 128;
+	if constexpr (sizeof(T) == 8 && E3D_FP64_RECON_VAR) {
+		if (v.tet4 && !first) {
+			k_recon_var<GRAD, LIM><<<(v.NR + RV_CELLS - 1) / RV_CELLS, 5 * RV_CELLS, 0, st>>>(v, ph);
+			return;
+		}
+	}
 	if (v.tet4) {
 		if (first) k_recon<T, GRAD, LIM, true, 4><<<grid, 128, 0, st>>>(v, ph, carry);
 		else k_recon<T, GRAD, LIM, false, 4><<<grid, 128, 0, st>>>(v, ph, carry);
