@@ -1,8 +1,10 @@
 // FP64 batch kernels built with fused multiply-add contraction (see the
 // Makefile).  They run the FP64 finishing phase of batched solves: the same
 // discrete equations as the bit-identical path, converging to the same
-// solution, with results that differ from it in the last bits.
+// solution, with results that differ from it in the last bits.  First-order
+// AUSM forms each cell's side quantities once (E3D_SHARED_SIDES, kernels.cuh).
 #define E3D_BATCH_NS batch_fast
+#define E3D_SHARED_SIDES
 #include "batch_launch.cuh"
 
 namespace e3d {

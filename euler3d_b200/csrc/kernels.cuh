@@ -269,6 +269,17 @@ __device__ __forceinline__ Q5<T> conservative_update(const double w0[5], T coef,
                                                      double wn[5]) {
 	for (int v = 0; v < 5; v++) wn[v] = w0[v] - (double)(coef) * (double)(rc[v] - rd[v]);
 	Q5<T> q;
+#ifdef E3D_SHARED_SIDES
+	if constexpr (sizeof(T) == 8) {  // contracted FP64 batch kernels: one reciprocal of rho
+		const double ir = 1.0 / wn[0];
+		q.r = wn[0];
+		q.u = wn[1] * ir;
+		q.v = wn[2] * ir;
+		q.w = wn[3] * ir;
+		q.p = gm1 * (wn[4] - 0.5 * (wn[1] * wn[1] + wn[2] * wn[2] + wn[3] * wn[3]) * ir);
+		return q;
+	}
+#endif
 	q.r = (T)wn[0];
 	q.u = (T)(wn[1] / wn[0]);
 	q.v = (T)(wn[2] / wn[0]);
@@ -476,6 +487,80 @@ __device__ __forceinline__ void load_geo(const T* __restrict__ a, const SlotRang
 }
 
 #define E3D_SLOTS(k, r) for (int k = 0; k < (NSL == 4 ? 4 : MAXSL); k++) if (NSL == 4 || k < r.n)
+
+// First-order AUSM with each cell's side quantities formed once (built only
+// where E3D_SHARED_SIDES is defined: the FP64 batch kernels with contraction,
+// which are not held to the reference's operation order).  The reference forms
+// a side's p/rho, speed of sound, enthalpy and c-scaled flux vector again in
+// every face flux, convective and dissipative alike (AusmScheme.cpp:716-871,
+// 102-243); a cell's own side is the same at all its faces, so here it is
+// formed once per cell and the neighbour's once per face, the normal Mach
+// number is V times 1/c, and c and 1/c come from one reciprocal square root.
+// Same formulas otherwise, including the branch tests.
+template <class T>
+struct AusmSide {
+	T u, v, w, p, ic;  // velocity, pressure, 1/c
+	T F[5];            // rho c (1, u, v, w, H)
+};
+template <class T>
+__device__ __forceinline__ AusmSide<T> ausm_side(const Q5<T>& q, T g, T gr) {
+	AusmSide<T> s;
+	const T pr = q.p / q.r;
+	const T x = g * pr;
+	s.ic = rsqrt(x);  // 1/c, and c = x/c: one reciprocal square root for both
+	const T c = x * s.ic;
+	const T H = T(0.5) * (q.u * q.u + q.v * q.v + q.w * q.w) + gr * pr;
+	s.u = q.u;
+	s.v = q.v;
+	s.w = q.w;
+	s.p = q.p;
+	s.F[0] = q.r * c;
+	s.F[1] = s.F[0] * q.u;
+	s.F[2] = s.F[0] * q.v;
+	s.F[3] = s.F[0] * q.w;
+	s.F[4] = s.F[0] * H;
+	return s;
+}
+template <class T, bool DISS>
+__device__ __forceinline__ void ausm_face_sides(const AusmSide<T>& L, const AusmSide<T>& R, T nx, T ny, T nz, T nn,
+                                                T fc[5], T fd[5]) {
+	const T ML = (L.u * nx + L.v * ny + L.w * nz) * L.ic;
+	const T MR = (R.u * nx + R.v * ny + R.w * nz) * R.ic;
+	T pLp, MLp, pRm, MRm;
+	if (ML <= T(-1.0)) {
+		pLp = T(0);
+		MLp = T(0);
+	} else if (ML < T(1.0)) {
+		MLp = T(0.25) * (ML + T(1.0)) * (ML + T(1.0));
+		pLp = L.p * MLp * (T(2.0) - ML);
+	} else {
+		MLp = ML;
+		pLp = L.p;
+	}
+	if (MR <= T(-1.0)) {
+		pRm = R.p;
+		MRm = MR;
+	} else if (MR < T(1.0)) {
+		MRm = T(-0.25) * (MR - T(1.0)) * (MR - T(1.0));
+		pRm = -R.p * MRm * (T(2.0) + MR);
+	} else {
+		pRm = T(0);
+		MRm = T(0);
+	}
+	const T M = MLp + MRm;
+	const T hM = T(0.5) * M * nn, ps = (pLp + pRm) * nn;
+	for (int k = 0; k < 5; k++) fc[k] = hM * (L.F[k] + R.F[k]);
+	fc[1] += nx * ps;
+	fc[2] += ny * ps;
+	fc[3] += nz * ps;
+	if (DISS) {
+		const T delta = T(0.25);
+		T Mf = M;
+		if (!(tabs(Mf) > delta)) Mf = (Mf * Mf + delta * delta) / (T(2.0) * delta);
+		const T ha = T(0.5) * tabs(Mf) * nn;
+		for (int k = 0; k < 5; k++) fd[k] = ha * (R.F[k] - L.F[k]);
+	}
+}
 
 // Pass 1 of a stage, one thread per real cell: gradient, limiter and MUSCL
 // face states of the cell and of its ghost cells.  FIRST additionally computes
@@ -806,6 +891,11 @@ __device__ __forceinline__ void flux_update_cell(const FusedView<T>& v, const Ph
 		qc = ld5(v.Pin, v.NA, c);
 		load_int<T, NSL>(v.slot_nbr, sr, nb);
 	}
+#ifdef E3D_SHARED_SIDES
+	constexpr bool shared_sides = ORDER1 && SCHEME == FLUX_AUSM;
+	AusmSide<T> own;
+	if constexpr (shared_sides) own = ausm_side(qc, g, gr);
+#endif
 	T geo[MAXSL][4];
 	load_geo<T, NSL>(v.sgeo, sr, geo);
 #pragma unroll
@@ -826,6 +916,13 @@ __device__ __forceinline__ void flux_update_cell(const FusedView<T>& v, const Ph
 			qv(R, q) = left ? qv(qn, q) : qv(qo, q);
 		}
 		T fc[5], fd[5];
+#ifdef E3D_SHARED_SIDES
+		if constexpr (shared_sides) {
+			const AusmSide<T> nbr = ausm_side(qn, g, gr);
+			if (left) ausm_face_sides<T, DISS>(own, nbr, geo[k][0], geo[k][1], geo[k][2], geo[k][3], fc, fd);
+			else ausm_face_sides<T, DISS>(nbr, own, geo[k][0], geo[k][1], geo[k][2], geo[k][3], fc, fd);
+		} else
+#endif
 		if (SCHEME == FLUX_ROE) {
 			flux_central(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], gr, fc);
 			if (DISS) flux_roe_diss(L, R, geo[k][0], geo[k][1], geo[k][2], geo[k][3], gr, gm1, fd);
