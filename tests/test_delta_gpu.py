@@ -20,10 +20,10 @@ from euler3d_b200 import meshgen as mg
 pytestmark = pytest.mark.gpu
 
 
-def _channel(tmp_path, name, n, mach, aoa, order=1, flux="ausm"):
+def _channel(tmp_path, name, n, mach, aoa, order=1, flux="ausm", blocks=1):
     d = mg.Deck(topology="", mach=mach, aoa_deg=aoa, stages=5, cfl=1.5, order=order, flux=flux,
                 gradient="greengauss", limiter="barthjespersen")
-    return api.Case(mg.write_case(str(tmp_path / name), n, 1, prefix=name, deck=d, sides="channel"))
+    return api.Case(mg.write_case(str(tmp_path / name), n, blocks, prefix=name, deck=d, sides="channel"))
 
 
 def _first_below(conv, level):
@@ -41,7 +41,8 @@ def _solve(cases, finish, crit):
 
 
 def test_difference_form_passes_the_fp32_floor_to_the_fp64_solution(tmp_path):
-    cases = [_channel(tmp_path, "a", 8, 0.5, 2.0), _channel(tmp_path, "b", 10, 0.72, -1.0)]
+    # the second case has 3 blocks: halo ghosts rebased from their origin cells
+    cases = [_channel(tmp_path, "a", 8, 0.5, 2.0), _channel(tmp_path, "b", 9, 0.72, -1.0, blocks=3)]
     bd, hd = _solve(cases, "fp32-delta", -10.0)
     bf, hf = _solve(cases, "fp64-fma", -10.0)
     for c in range(len(cases)):
@@ -52,10 +53,11 @@ def test_difference_form_passes_the_fp32_floor_to_the_fp64_solution(tmp_path):
             assert abs(hd[c][col][-1] - hf[c][col][-1]) <= 1e-9 * max(abs(hf[c][col][-1]), 1e-2), col
     # the full state is readable in difference form and equals the FP64 solve's
     # converged state to the same accuracy
-    for c in range(len(cases)):
-        nr, na = cases[c].block_info(0).n_real, cases[c].block_info(0).n_all
-        pd = bd.get(c, "prim").reshape(5, na)[:, :nr]
-        pf = bf.get(c, "prim").reshape(5, na)[:, :nr]
+    for blk in range(bd.n_blocks):
+        case, local = (cases[0], 0) if blk == 0 else (cases[1], blk - 1)
+        nr, na = case.block_info(local).n_real, case.block_info(local).n_all
+        pd = bd.get(blk, "prim").reshape(5, na)[:, :nr]
+        pf = bf.get(blk, "prim").reshape(5, na)[:, :nr]
         assert np.max(np.abs(pd - pf) / np.abs(pf).clip(1e-2)) < 1e-8
     bd.close()
     bf.close()
