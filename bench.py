@@ -354,7 +354,7 @@ def warmstart_bounded(n_cases: int = 4, n_max: int = 32) -> dict:
     first `n_cases` held-out cases of the warm-start sweep with at most n_max^3
     x 6 tetrahedra, solved by the plain FP64 drop-in path case after case and
     by one batch with the committed surrogate's warm start (FP32 to -5, then
-    contracted FP64).  The same per-case stop rule and reference residual as
+    FP32 in difference form on an FP64 base).  The same per-case stop rule and reference residual as
     `--workload warmstart`, on fewer and smaller cases."""
     from euler3d_b200 import api
     from euler3d_b200 import sweep as sw

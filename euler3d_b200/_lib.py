@@ -18,6 +18,7 @@ ERRORS = {
     -1: "E3D_ERR_ARG", -2: "E3D_ERR_IO", -3: "E3D_ERR_FORMAT", -4: "E3D_ERR_MESH", -5: "E3D_ERR_CUDA",
     -6: "E3D_ERR_NONFINITE", -7: "E3D_ERR_STATE", -9: "E3D_ERR_LIMIT",
 }
+ERRORS_BY_NAME = {v: k for k, v in ERRORS.items()}
 GRAD = {"greengauss": 0, "leastsquares": 1}
 LIM = {"barthjespersen": 0, "venkatakrishnan": 1}
 FLUX = {"roe": 0, "ausm": 1}

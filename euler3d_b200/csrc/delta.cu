@@ -106,6 +106,7 @@ __device__ __forceinline__ void side_flux(const DCell& s, float F[5], float dF[5
 // the difference is summed through them, so every term stays a difference.
 template <class P>
 __device__ __forceinline__ float piecewise_delta(float x, float d, float lo, float hi, int i0, int i1, P piece) {
+	if (i0 == i1) return piece(i0, x, d);
 	float acc = 0.f, x0 = x, rest = d;
 	if (i1 > i0) {
 		for (int i = i0; i < i1; i++) {
@@ -233,8 +234,11 @@ __global__ void __launch_bounds__(128) k_delta_start_tiles(FusedView<float> v, P
 
 // one RK stage: flux differences, residual, conserved-difference update,
 // primitive differences and the boundary ghosts' differences
+#ifndef E3D_DELTA_MIN_BLOCKS
+#define E3D_DELTA_MIN_BLOCKS 5
+#endif
 template <bool DISS>
-__global__ void __launch_bounds__(128, 5) k_delta_flux_tiles(FusedView<float> v, Physics ph, float alpha, float beta,
+__global__ void __launch_bounds__(128, E3D_DELTA_MIN_BLOCKS) k_delta_flux_tiles(FusedView<float> v, Physics ph, float alpha, float beta,
                                                              int last, const int4* __restrict__ work) {
 	const int4 t = work[blockIdx.x];
 	const int c = t.x + threadIdx.x;
@@ -260,8 +264,9 @@ __global__ void __launch_bounds__(128, 5) k_delta_flux_tiles(FusedView<float> v,
 		const DCell nbr = dcell(ld5(v.Pb, v.NA, nb[k]), ld5(v.Pin, v.NA, nb[k]), g, gr);
 		const float4 n = geo[k];
 		float fc[5], fd[5];
-		if (left) ausm_delta_face<DISS>(own, nbr, n.x, n.y, n.z, n.w, fc, fd);
-		else ausm_delta_face<DISS>(nbr, own, n.x, n.y, n.z, n.w, fc, fd);
+		// one call with the sides selected by value: a branch on the orientation
+		// would run the face arithmetic twice in warps whose cells differ
+		ausm_delta_face<DISS>(left ? own : nbr, left ? nbr : own, n.x, n.y, n.z, n.w, fc, fd);
 		if (left) {
 #pragma unroll
 			for (int q = 0; q < 5; q++) {

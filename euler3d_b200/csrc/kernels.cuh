@@ -919,8 +919,10 @@ __device__ __forceinline__ void flux_update_cell(const FusedView<T>& v, const Ph
 #ifdef E3D_SHARED_SIDES
 		if constexpr (shared_sides) {
 			const AusmSide<T> nbr = ausm_side(qn, g, gr);
-			if (left) ausm_face_sides<T, DISS>(own, nbr, geo[k][0], geo[k][1], geo[k][2], geo[k][3], fc, fd);
-			else ausm_face_sides<T, DISS>(nbr, own, geo[k][0], geo[k][1], geo[k][2], geo[k][3], fc, fd);
+			// sides selected by value: a branch on the orientation would run the
+			// face arithmetic twice in warps whose cells differ
+			ausm_face_sides<T, DISS>(left ? own : nbr, left ? nbr : own, geo[k][0], geo[k][1], geo[k][2], geo[k][3],
+			                         fc, fd);
 		} else
 #endif
 		if (SCHEME == FLUX_ROE) {

@@ -21,6 +21,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from . import _lib as L
 from . import api
 from . import meshgen as mg
 
@@ -86,7 +87,7 @@ def solve_plain(case: api.Case, criterion: float, max_iter: int, check_every: in
 
 def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrogate: api.Surrogate | None = None,
                   switch_at: float | None = -5.0, iters_per_launch: int = 50, stall_window: int = 400,
-                  fp64: str = "fp64-fma") -> dict:
+                  fp64: str = "auto") -> dict:
     """All cases in one batch: one freestream iteration (the reference residual
     of each case's drop), the surrogate's warm start when given, FP32
     iterations to `switch_at` (below a 4-order drop, a case whose FP32
@@ -94,12 +95,15 @@ def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrog
     rounding floor, also moves on),
     then the finishing phase to `criterion` (`fp64`: "fp64-fma" for the FP64
     kernels built with fused multiply-add, "fp64" for the bit-identical ones,
-    "fp32-delta" for FP32 iterations in difference form on an FP64 base); each
+    "fp32-delta" for FP32 iterations in difference form on an FP64 base,
+    "auto" for the difference form where the scheme has it (first-order AUSM
+    on tetrahedra; the fastest form there) and contracted FP64 elsewhere); each
     case leaves the work list once it gets there."""
     t0 = time.perf_counter()
     b = api.Batch(cases, precision="fp32" if switch_at is not None else "fp64",
                   hist_capacity=max(4096, iters_per_launch * 4))
-    if switch_at is None and fp64 == "fp64-fma":
+    if switch_at is None and fp64 in ("fp64-fma", "auto"):
+        fp64 = "fp64-fma"
         api.set_precision(b, fp64)
     t_setup = time.perf_counter() - t0
     t0 = time.perf_counter()
@@ -119,7 +123,17 @@ def solve_batched(cases: list[api.Case], criterion: float, max_iter: int, surrog
         b.solve_batch(max_iter, switch_at, iters_per_launch=iters_per_launch, stall_window=stall_window)
         phases.append(dict(precision="fp32", to=switch_at, wall_s=time.perf_counter() - tp, tuning=b.tuning()))
         tp = time.perf_counter()
-        api.set_precision(b, fp64)
+        if fp64 == "auto":
+            try:
+                api.set_precision(b, "fp32-delta")
+                fp64 = "fp32-delta"
+            except L.E3DError as e:
+                if e.code != L.ERRORS_BY_NAME["E3D_ERR_ARG"]:
+                    raise
+                fp64 = "fp64-fma"
+                api.set_precision(b, fp64)
+        else:
+            api.set_precision(b, fp64)
         phases.append(dict(precision="switch", wall_s=time.perf_counter() - tp))
     tp = time.perf_counter()
     b.solve_batch(max_iter, criterion, iters_per_launch=iters_per_launch)
