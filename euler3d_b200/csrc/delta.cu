@@ -69,10 +69,11 @@ __device__ __forceinline__ DCell dcell(const Q5<float>& b, const Q5<float>& d, f
 	const float dpr = (d.p - pr * d.r) / (b.r + d.r);  // p'/r' - p/r
 	s.H = 0.5f * qq + gr * pr;
 	s.dH = 0.5f * dqq + gr * dpr;
-	const float c = sqrtf(g * pr), c1 = sqrtf(g * (pr + dpr));
+	const float x = g * pr, x1 = g * (pr + dpr);
+	s.ic = rsqrtf(x);  // 1/c, and c = x/c: one reciprocal square root for both
+	s.ic1 = rsqrtf(x1);
+	const float c = x * s.ic, c1 = x1 * s.ic1;
 	s.dc = g * dpr / (c + c1);
-	s.ic = 1.f / c;
-	s.ic1 = 1.f / c1;
 	s.F1 = b.r * c;
 	s.dF1 = d.r * c1 + b.r * s.dc;
 	return s;

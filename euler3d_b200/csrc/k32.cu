@@ -1,6 +1,6 @@
-// FP32 instantiations of the fused path (multiply-add contraction allowed).
+// FP32 instantiations of the single-case fused path (multiply-add contraction
+// allowed); the FP32 batch kernels are in k32b.cu.
 #include "launch_common.cuh"
-#include "batch_launch.cuh"
 
 namespace e3d {
 
@@ -13,11 +13,5 @@ template void launch_start<float>(const FusedView<float>&, const Physics&, int, 
 template void launch_flux_update<float>(const FusedView<float>&, const Physics&, int, bool, double, double, int, int,
                                         cudaStream_t);
 
-template int batch::persistent_blocks_per_sm<float>(int, int, int, bool);
-template cudaError_t batch::launch_persistent<float>(const FusedView<float>&, const FusedView<float>&, const Physics&,
-                                              const PersistArgs&, int, int, int, bool, int, cudaStream_t);
-
-template cudaError_t batch::launch_tiled_iterations<float>(const FusedView<float>&, const FusedView<float>&, const Physics&,
-                                                    const PersistArgs&, int, int, int, bool, cudaStream_t);
 
 }  // namespace e3d
