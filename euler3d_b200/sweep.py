@@ -316,13 +316,14 @@ def finishing_forms(n: int = 48, count: int = 8, iters: int = 300, depth_cases: 
                 rec["forms"][form] = dict(ms_per_iter=ms / iters, cell_iters_per_s=cells * iters / (ms / 1e3))
             b.close()
             sub = cases[:depth_cases]
-            a = solve_batched(sub, depth, 200000, switch_at=None, fp64="fp64-fma")
-            d = solve_batched(sub, depth, 200000, switch_at=-5.0, fp64="fp32-delta")
-            rec["depth"] = dict(level=depth, fp64_fma=a, fp32_then_delta=d,
-                                max_rel_dcl=max(abs(x["cl"] - y["cl"]) / abs(y["cl"])
-                                                for x, y in zip(d["cases"], a["cases"])),
-                                max_rel_dcd=max(abs(x["cd"] - y["cd"]) / abs(y["cd"])
-                                                for x, y in zip(d["cases"], a["cases"])))
+            if sub:
+                a = solve_batched(sub, depth, 200000, switch_at=None, fp64="fp64-fma")
+                d = solve_batched(sub, depth, 200000, switch_at=-5.0, fp64="fp32-delta")
+                rec["depth"] = dict(level=depth, fp64_fma=a, fp32_then_delta=d,
+                                    max_rel_dcl=max(abs(x["cl"] - y["cl"]) / abs(y["cl"])
+                                                    for x, y in zip(d["cases"], a["cases"])),
+                                    max_rel_dcd=max(abs(x["cd"] - y["cd"]) / abs(y["cd"])
+                                                    for x, y in zip(d["cases"], a["cases"])))
             for c in cases:
                 c.close()
     finally:
@@ -341,6 +342,9 @@ def main(argv=None) -> int:
     ap.add_argument("--out", default=None)
     ap.add_argument("--cases", type=int, default=None)
     ap.add_argument("--steps", type=int, default=40000)
+    ap.add_argument("--n", type=int, default=48, help="finishing: hexahedra per side of each case")
+    ap.add_argument("--iters", type=int, default=300, help="finishing: timed iterations per form")
+    ap.add_argument("--depth-cases", type=int, default=2, help="finishing: cases of the depth check (0: none)")
     a = ap.parse_args(argv)
     if a.command == "train":
         if not a.out:
@@ -349,7 +353,7 @@ def main(argv=None) -> int:
     elif a.command == "wing":
         info = wing_warmstart(n_train=a.cases or 32, out=a.out)
     else:
-        info = finishing_forms(count=a.cases or 8)
+        info = finishing_forms(n=a.n, count=a.cases or 8, iters=a.iters, depth_cases=a.depth_cases)
     print(json.dumps(info))
     return 0
 
