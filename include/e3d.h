@@ -281,7 +281,10 @@ int e3d_shard_push_flow_data(e3d_solver* s, const double* all_blocks, int n_iter
  * First-order AUSM on all-tetrahedron meshes; E3D_ERR_ARG otherwise.  In this
  * form only e3d_batch_solve, e3d_history / e3d_batch_case_history, reading
  * "prim" and "w0" (the full state), and a further switch to E3D_FP64 or
- * E3D_FP64_FMA are available; other calls return E3D_ERR_STATE.
+ * E3D_FP64_FMA are available; other calls return E3D_ERR_STATE (E3D_FP32
+ * leaves the solver in difference form).  Memory: 5 floats per cell and 5
+ * doubles per cell of base state, 10 floats per real cell of differences and
+ * base residual.
  * e3d_cell_features: surrogate inputs of every real cell of every case, in
  * device cell order (blocks in order, real cells in the order that
  * e3d_options.renumber chose; file order by default), 8 floats per

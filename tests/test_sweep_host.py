@@ -43,3 +43,61 @@ def test_first_below_counts_iterations_like_the_stop_test():
     assert sw._first_below(conv, -8.0) == 4  # the 4th iteration is the first at or below -8
     assert sw._first_below(conv, -9.0) == 6
     assert sw._first_below(conv, -10.0) is None
+
+
+class _FakeBatch:
+    """Stands in for api.Batch on a host without a GPU: records the solve calls."""
+
+    def __init__(self, cases, precision="fp32", hist_capacity=4096):
+        self.cases, self.precision, self.calls = cases, precision, []
+
+    def solve_batch(self, max_iter, criterion, iters_per_launch=10, stall_window=0):
+        self.calls.append((self.precision, criterion))
+        return np.zeros(len(self.cases), dtype=np.int32), 1.0
+
+    def tuning(self):
+        return {"mode": "per-pass"}
+
+    def case_history(self, c):
+        return {"conv": np.array([[0.0] * 5, [-9.0] * 5]), "cl": np.array([0.1, 0.1]), "cd": np.array([0.01, 0.01])}
+
+    def close(self):
+        pass
+
+
+def _fake_set_precision(supports_delta, code=-1):
+    from euler3d_b200 import _lib as L
+
+    def set_precision(b, precision):
+        if precision == "fp32-delta" and not supports_delta:
+            raise L.E3DError(code, "the difference form covers first-order AUSM")
+        b.precision = precision
+
+    return set_precision
+
+
+def test_finishing_form_is_the_difference_form_where_the_scheme_has_one(monkeypatch):
+    monkeypatch.setattr(sw.api, "Batch", _FakeBatch)
+    monkeypatch.setattr(sw.api, "set_precision", _fake_set_precision(True))
+    r = sw.solve_batched(["a", "b"], -8.0, 100)
+    assert [p["precision"] for p in r["phases"]] == ["fp32", "switch", "fp32-delta"]
+    monkeypatch.setattr(sw.api, "set_precision", _fake_set_precision(False))
+    r = sw.solve_batched(["a", "b"], -8.0, 100)
+    assert [p["precision"] for p in r["phases"]] == ["fp32", "switch", "fp64-fma"]
+    r = sw.solve_batched(["a"], -8.0, 100, fp64="fp64")  # an explicit form is used as given
+    assert r["phases"][-1]["precision"] == "fp64"
+    r = sw.solve_batched(["a"], -8.0, 100, switch_at=None)  # FP64 from the start
+    assert [p["precision"] for p in r["phases"]] == ["fp64"]
+
+
+def test_finishing_form_selection_passes_other_errors_on(monkeypatch):
+    from euler3d_b200 import _lib as L
+
+    monkeypatch.setattr(sw.api, "Batch", _FakeBatch)
+    monkeypatch.setattr(sw.api, "set_precision", _fake_set_precision(False, code=-5))
+    try:
+        sw.solve_batched(["a"], -8.0, 100)
+    except L.E3DError as e:
+        assert e.code == -5
+    else:
+        raise AssertionError("a CUDA error from the switch must not fall back silently")
