@@ -498,8 +498,9 @@ void Engine::count_device_bytes() {
 	                &f64_.lsw, &f64_.vol})
 		bytes += b->n * sizeof(double);
 	for (auto* b : {&f32_.P0, &f32_.P1, &f32_.FS, &f32_.Rc, &f32_.Rd, &f32_.dt, &f32_.sgeo, &f32_.sS, &f32_.srv,
-	                &f32_.lsw, &f32_.vol})
+	                &f32_.lsw, &f32_.vol, &Pb32_, &dW_, &Rb_})
 		bytes += b->n * sizeof(float);
+	bytes += Pb64_.n * sizeof(double);
 	dev_bytes_ = bytes;
 }
 
