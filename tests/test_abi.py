@@ -36,3 +36,15 @@ def test_version_and_error_text():
     rc = lib.e3d_case_load(b"/nonexistent/deck", None, ctypes.byref(h))
     assert rc == -2
     assert b"nonexistent" in lib.e3d_last_error()
+
+
+def test_precision_constants_match_the_header():
+    src = open(os.path.join(REPO, "include", "e3d.h")).read()
+    for name, value in (("E3D_FP64", _lib.FP64), ("E3D_FP32", _lib.FP32), ("E3D_FP64_FMA", _lib.FP64_FMA),
+                        ("E3D_FP32_DELTA", _lib.FP32_DELTA)):
+        m = re.search(rf"#define {name} (\d+)", src)
+        assert m and int(m.group(1)) == value, name
+    lib = _lib.lib()
+    assert lib.e3d_solver_set_precision(None, _lib.FP32_DELTA) == -1  # null solver: an error, not a crash
+    assert b"null solver" in lib.e3d_last_error()
+    assert lib.e3d_solver_set_precision(None, 7) == -1
